@@ -1,0 +1,347 @@
+"""Benchmark of the fused DG-SEM Maxwell LSRK45 path (libnwb) on B200.
+
+Workload (one GPU): periodic box [0,1]^3, 32x32x32 hexahedra, 8 GLL points per
+direction (order 7, 16.8 M nodes x 6 fields = 100.7 M DOF), central flux, CFL
+0.5, Gaussian pulse Ez = exp(-|r-r0|^2/sigma^2), sigma = 0.1, r0 ~ U[0.3,0.7]^3
+from the seed.  A "step" is one LSRK45 time step (five fused stage launches).
+
+metric: GDOF-stage/s = 6 * npts * 5 * steps / seconds / 1e9.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+  python bench.py --impl reference ...   # the reference's own CPU implementation
+
+With --gpus N > 1 (under torchrun) every rank advances its own independent
+cavity (replicas, weak scaling, no data-path collective); the timing is the
+maximum over ranks and ``value`` is the sum of all ranks' DOF-stages over it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GDOF-stage/s"
+WORKLOAD = dict(workload="periodic_box_32x32x32_N8_central", nel=(32, 32, 32), N=8,
+                periodic=True, c0=0.0, cfl=0.5, sigma=0.1)
+BYTES_PER_DOF_STAGE = 32  # FP64 u and k, each read and written once
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["nwb", "reference"], default="nwb")
+    p.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    return p.parse_args()
+
+
+def initial_state(x, y, z, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r0 = rng.uniform(0.3, 0.7, 3)
+    n = x.size
+    u = np.zeros(6 * n)
+    s2 = WORKLOAD["sigma"] ** 2
+    u[2 * n:3 * n] = np.exp(-((x - r0[0]) ** 2 + (y - r0[1]) ** 2 + (z - r0[2]) ** 2) / s2)
+    return u
+
+
+# ---- clocks ------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [c.strip() for c in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "samples": len(rows),
+                "reasons": sorted(reasons)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per stage launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d
+    except (OSError, ValueError):
+        return None
+
+
+# ---- CPU baseline: the reference's own implementation on the host cores ---------------
+def cpu_reference_rate(seconds_target=15.0, seed=0):
+    """Times the reference's RHS + LSRK45 (its kernel bodies compiled for the host,
+    oracle/_ref) -- or, if that build is absent, the oracle port -- on a bounded sample
+    of the workload: the same element order, flux and pulse on an 8x8x8-element
+    periodic sub-box (1/64 of the mesh), whole LSRK45 steps."""
+    from oracle import oracle as O
+    nel = (8, 8, 8)
+    N = WORKLOAD["N"]
+    kind = "reference" if O.ref_available() else "port"
+    if kind == "reference":
+        m = O.ref_box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
+        dx = m.dxmin_ref
+        stepper = O.ref_step
+        cores = O.ref().nwref_threads()
+    else:
+        m = O.box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
+        dx = O.dxmin(m)
+        stepper = O.step
+        cores = O.threads()
+    u = initial_state(m.x * 4, m.y * 4, m.zc * 4, seed)
+    dt = WORKLOAD["cfl"] * dx
+    t0 = time.perf_counter()
+    u, k = stepper(m, WORKLOAD["c0"], dt, 1, u)
+    one = time.perf_counter() - t0
+    nsteps = max(1, int(seconds_target / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    stepper(m, WORKLOAD["c0"], dt, nsteps, u, k)
+    sec = time.perf_counter() - t0
+    dof_stage = 6 * m.npts * 5 * nsteps
+    return dict(value=dof_stage / sec / 1e9, unit=METRIC, cores=int(cores), kind=kind,
+                sample=f"{nsteps} LSRK45 steps on an 8x8x8-element periodic sub-box, N=8 "
+                       f"({m.npts} nodes), {sec:.1f} s on {cores} host threads",
+                seconds=sec, steps=nsteps, npts=m.npts)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation (oracle/_ref)."""
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    N = WORKLOAD["N"]
+    nel = (8, 8, 8)
+    if kind == "reference":
+        m = O.ref_box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
+        dx, stepper, cores = m.dxmin_ref, O.ref_step, O.ref().nwref_threads()
+    else:
+        m = O.box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
+        dx, stepper, cores = O.dxmin(m), O.step, O.threads()
+    u = initial_state(m.x * 4, m.y * 4, m.zc * 4, args.seed)
+    k = np.zeros_like(u)
+    dt = WORKLOAD["cfl"] * dx
+    for _ in range(args.warmup):
+        u, k = stepper(m, WORKLOAD["c0"], dt, 1, u, k)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        u, k = stepper(m, WORKLOAD["c0"], dt, 1, u, k)
+        times.append(time.perf_counter() - t0)
+    sec = sum(times)
+    value = 6 * m.npts * 5 * args.steps / sec / 1e9
+    sample = (f"each step: one LSRK45 step on an 8x8x8-element periodic sub-box of the "
+              f"workload, N=8 ({m.npts} nodes)")
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload=WORKLOAD["workload"], N=N, nel=list(WORKLOAD["nel"]),
+                           flux="central", cfl=WORKLOAD["cfl"], sample_nel=list(nel)),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": int(cores), "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from nekwave_b200 import DgSolver, Mesh
+
+    torch.cuda.set_device(local)
+    dist_on = world > 1
+    if dist_on:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist_on:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    N = WORKLOAD["N"]
+    mesh = Mesh(N)
+    mesh.createBoxMesh(*WORKLOAD["nel"], 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, True, True, True)
+    npts = mesh.getTotalPoints()
+    dt = WORKLOAD["cfl"] * mesh.computeMinNodeDistance()
+    u0 = initial_state(mesh.getCoordX(), mesh.getCoordY(), mesh.getCoordZ(), args.seed + rank)
+    solver = DgSolver(args.precision)
+    solver.initialize(mesh, WORKLOAD["c0"])
+    solver.uploadState(u0)
+    info = solver.info()
+
+    # warm-up (graphs captured here)
+    solver.steps(dt, args.warmup)
+    barrier()
+
+    # ---- timed region: K steps, inputs resident in HBM (3 x 805 MB > L2) ---------------
+    launches0 = solver.launchCount()
+    with ClockSampler(local) as clk:
+        barrier()
+        ms = solver.timeSteps(dt, args.steps, graph=True)
+        barrier()
+    launches = solver.launchCount() - launches0
+    clocks = clk.summary()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist_on:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    dof_stage = 6 * npts * 5 * args.steps * world
+    value = dof_stage / (ms_max / 1e3) / 1e9
+
+    # ---- roofline of the fused stage kernel (CUDA events on the solver's stream) ----------
+    stage_ms = solver.timeStageKernel(dt, 50)
+    alg_bytes = BYTES_PER_DOF_STAGE * 6 * npts
+    achieved = alg_bytes / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    tr = profiled_traffic()
+    traffic = None
+    if tr and tr.get("npts") and tr.get("precision", "fp64") == args.precision:
+        traffic = tr["dram_bytes_per_launch"] * npts / tr["npts"]
+
+    # ---- end to end through the public API, host buffers, copies inside the timed region --
+    import ctypes
+    host = torch.empty(6 * npts, dtype=torch.float64).pin_memory()
+    host.copy_(torch.from_numpy(u0))
+    hnp = host.numpy()
+    barrier()
+    t0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = args.e2e_steps
+    for _ in range(e2e_steps):
+        solver.uploadState(hnp)            # H2D of the step's input state (pinned)
+        solver.step(dt, 0.0)               # one LSRK45 step (blocking, as the reference)
+        solver.downloadState(hnp)          # D2H of the step's result state
+    barrier()
+    e2e_sec = time.perf_counter() - t0
+    tt = torch.tensor([e2e_sec], dtype=torch.float64, device="cuda")
+    if dist_on:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = 6 * npts * 5 * e2e_steps * world / float(tt.item()) / 1e9
+    del ctypes, ev0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate()
+
+    if dist_on:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
+            "data": "synthetic (seeded Gaussian pulse)",
+            "config": dict(workload=WORKLOAD["workload"], N=N, order=N - 1,
+                           nel=list(WORKLOAD["nel"]), npts=npts, dof=6 * npts,
+                           flux="central", cfl=WORKLOAD["cfl"], dt=dt,
+                           precision=args.precision, parallelism=f"replicas x{world}",
+                           l2="inputs larger than L2 (u_in, u_out, k: 3 x 805 MB)",
+                           kernel=dict(ks=info["ks"], epb=info["epb"],
+                                       threads=info["threads_per_block"],
+                                       smem=info["smem_bytes"], geometry=info["geometry"])),
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "kernel": "stage_kernel",
+                         "stage_ms": stage_ms, "alg_bytes_per_launch": alg_bytes},
+            "e2e": {"value": e2e_value, "unit": METRIC,
+                    "h2d_bytes_per_step": 6 * npts * 8, "d2h_bytes_per_step": 6 * npts * 8,
+                    "steps": e2e_steps,
+                    "pattern": "uploadState (pinned) + step + downloadState per step"},
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    solver.finalize()
+    if dist_on:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

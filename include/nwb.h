@@ -1,0 +1,155 @@
+/*
+ * nwb.h -- C ABI of libnwb, the B200-native (sm_100a) DG-SEM Maxwell right-hand
+ * side and LSRK45 time step of NekWave.
+ *
+ * The library is a drop-in for the reference's DgSolver (src/dg_solver.hpp:35-102)
+ * and the single-rank kernel launchers behind it (src/device/dg_kernels.hpp:13-88):
+ * it takes the same mesh arrays DgSolver::initialize reads from Mesh
+ * (src/dg_solver.cpp:40-241), the same SoA state [Ex,Ey,Ez,Hx,Hy,Hz][npts], and
+ * advances it with the same method.  Signatures use plain pointers and sizes only.
+ *
+ * Errors: every entry point returns an nwb_status.  nwb_last_error() gives a
+ * thread-local message for the last failure on the calling thread.  The
+ * reference aborts on any CUDA error (src/device/gpu_runtime.hpp:146-153); the
+ * DgSolver shim in nekwave_b200/ref_shim/ keeps that behaviour on top of these
+ * status codes.
+ *
+ * Terms: N is the number of GLL points per direction (the reference's Mesh::getN,
+ * polynomial degree N-1); nelt the number of hexahedral elements; npts = nelt*N^3;
+ * nfp = 6*N*N*nelt face points.
+ */
+#ifndef NWB_H
+#define NWB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NWB_VERSION 1
+
+typedef enum nwb_status {
+    NWB_OK = 0,
+    NWB_EINVAL = 1,      /* bad argument, size mismatch, unsupported mesh        */
+    NWB_ENOMEM = 2,      /* device or host allocation failed                      */
+    NWB_ECUDA = 3,       /* a CUDA runtime call failed                            */
+    NWB_ETIMEOUT = 4,    /* a bounded device wait gave up                         */
+    NWB_ENONFINITE = 5,  /* the state holds NaN or Inf                            */
+    NWB_EBUSY = 6,       /* admission refused: over the memory budget / no slot   */
+    NWB_ENOTFOUND = 7    /* unknown request or instance id                        */
+} nwb_status;
+
+typedef enum nwb_precision {
+    NWB_FP64 = 0,        /* all arithmetic in FP64 (the reference's precision)     */
+    NWB_FP32_BULK = 1    /* volume and flux arithmetic in FP32; solution, LSRK      */
+                         /* register, geometry, inverse mass and energy in FP64    */
+} nwb_precision;
+
+/* Mesh arrays exactly as the reference's DgSolver::initialize consumes them
+ * (src/dg_solver.cpp:76-112, 141-205).  All pointers are host pointers and are
+ * only read during nwb_solver_create.  Face points must be in the reference's
+ * canonical order: element-major, faces 0..5, then q, then p
+ * (Mesh::setupFaceData, src/mesh.cpp:985-1080) -- the order createBoxMesh
+ * produces; vol_idx_minus[fp] must equal Mesh::getFaceNodeVolIndex(e,f,p,q)
+ * (src/mesh.cpp:955-981). */
+typedef struct nwb_mesh_desc {
+    int N;                        /* GLL points per direction, 2..10               */
+    int nelt;                     /* number of elements                            */
+    const double* D;              /* [N*N] column-major, Mesh::getD                */
+    const double* w3;             /* [N^3] Mesh::getW3                             */
+    const double* jac;            /* [npts] Mesh::getJac                           */
+    const double* met[9];         /* [npts] each: rx,sx,tx,ry,sy,ty,rz,sz,tz       */
+    const int* vol_idx_minus;     /* [nfp] FacePointData::volIdxMinus              */
+    const int* vol_idx_plus;      /* [nfp] FacePointData::volIdxPlus (-1: none)    */
+    const int* bc_type;           /* [nfp] 0 interior/periodic, 1 PEC, 2 PMC       */
+                                  /* (nonzero is a PEC mirror, as the reference's */
+                                  /* flux kernel does, src/device/dg_kernels.cu:244) */
+    const double* nx;             /* [nfp] outward unit normal                     */
+    const double* ny;
+    const double* nz;
+    const double* dA;             /* [nfp] surface metric J_face w_p w_q           */
+} nwb_mesh_desc;
+
+typedef struct nwb_solver nwb_solver;
+typedef struct nwb_box_mesh nwb_box_mesh;
+
+/* ---- errors / version ------------------------------------------------------ */
+const char* nwb_last_error(void);
+const char* nwb_status_string(nwb_status s);
+int nwb_version(void);
+
+/* ---- box mesh builder ---------------------------------------------------------
+ * Replaces Mesh::createBoxMesh (src/mesh.cpp:683-843) with its geometry
+ * (src/mesh.cpp:188-314) and face data (src/mesh.cpp:985-1080), built with
+ * structural O(faces*N^2) connectivity instead of coordinate matching.
+ * periodic_mask: bit 0 = x, bit 1 = y, bit 2 = z.  The mesh owns host arrays
+ * that nwb_box_mesh_desc exposes through an nwb_mesh_desc. */
+nwb_status nwb_box_mesh_create(int N, int nelx, int nely, int nelz,
+                               double xmin, double xmax, double ymin, double ymax,
+                               double zmin, double zmax, int periodic_mask,
+                               nwb_box_mesh** out);
+nwb_status nwb_box_mesh_desc(const nwb_box_mesh* m, nwb_mesh_desc* out);
+/* Node coordinates [npts] each (Mesh::getCoordX/Y/Z) and GLL nodes/weights [N]. */
+nwb_status nwb_box_mesh_coords(const nwb_box_mesh* m, const double** x,
+                               const double** y, const double** z);
+nwb_status nwb_box_mesh_gll(const nwb_box_mesh* m, const double** z, const double** w);
+/* Smallest GLL node spacing, Mesh::computeMinNodeDistance (src/mesh.cpp:883-930). */
+nwb_status nwb_box_mesh_dxmin(const nwb_box_mesh* m, double* dxmin);
+void nwb_box_mesh_destroy(nwb_box_mesh* m);
+
+/* ---- single-mesh solver: DgSolver (src/dg_solver.hpp:35-102) -----------------
+ * nwb_solver_create     <- DgSolver::initialize(mesh, c0)   (src/dg_solver.cpp:40)
+ * nwb_upload_state      <- DgSolver::uploadState            (src/dg_solver.cpp:243)
+ * nwb_download_state    <- DgSolver::downloadState          (src/dg_solver.cpp:264)
+ * nwb_step              <- DgSolver::step, nsteps times     (src/dg_solver.cpp:306)
+ * nwb_solver_destroy    <- DgSolver::finalize               (src/dg_solver.cpp:529)
+ * c0 = 0 central flux, 1 upwind (src/device/dg_kernels.cu:206-212).
+ * The solver runs on the current CUDA device, on its own stream. */
+nwb_status nwb_solver_create(const nwb_mesh_desc* mesh, double c0,
+                             nwb_precision precision, nwb_solver** out);
+/* n must be 6*npts (the reference asserts the same, src/dg_solver.cpp:244). */
+nwb_status nwb_upload_state(nwb_solver* s, const double* host_state, size_t n);
+nwb_status nwb_download_state(nwb_solver* s, double* host_state, size_t n);
+/* Enqueues nsteps LSRK45 steps of size dt on the solver's stream and returns
+ * without waiting (the reference's step blocks; nwb_sync restores that). */
+nwb_status nwb_step(nwb_solver* s, double dt, int nsteps);
+nwb_status nwb_sync(nwb_solver* s);
+/* Right-hand side M^{-1}(K u + F*) of the current state into host memory [6*npts]:
+ * the quantity the reference's kernels leave in d_rhs_ before the LSRK update
+ * (src/dg_solver.cpp:487).  Does not change the state. */
+nwb_status nwb_eval_rhs(nwb_solver* s, double* host_rhs, size_t n);
+/* Discrete energy 1/2 sum J w_i w_j w_k (|E|^2+|H|^2) of the current state,
+ * FP64, on the device (src/case.cpp:733-766).  Returns NWB_ENONFINITE (and the
+ * non-finite energy) when the state holds NaN/Inf. */
+nwb_status nwb_energy(nwb_solver* s, double* energy);
+nwb_status nwb_solver_destroy(nwb_solver* s);
+
+/* Introspection used by tests and the benchmark. */
+typedef struct nwb_solver_info {
+    int N, nelt;
+    long long npts, stride;       /* component stride of the device state          */
+    int geometry;                 /* 0 axis-aligned affine, 1 affine, 2 per-node   */
+    int precision;
+    int ks, epb;                  /* threads per node column, elements per block   */
+    int threads_per_block;
+    int smem_bytes;
+    long long device_bytes;       /* device memory the solver holds                */
+} nwb_solver_info;
+nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info);
+/* Device pointer of the current state ([6][stride] doubles) and the solver's
+ * CUDA stream (a cudaStream_t), for callers that keep data on the device. */
+nwb_status nwb_solver_device_state(nwb_solver* s, double** d_state, void** stream);
+/* Number of kernels the solver has launched since it was created. */
+nwb_status nwb_solver_launch_count(const nwb_solver* s, long long* count);
+/* Times nsteps steps on the device with CUDA events on the solver's stream;
+ * *ms receives the elapsed device time.  use_graph replays CUDA graphs. */
+nwb_status nwb_time_steps(nwb_solver* s, double dt, int nsteps, int use_graph, float* ms);
+/* Per-stage-kernel average device time over nstages stage launches (ms). */
+nwb_status nwb_time_stage_kernel(nwb_solver* s, double dt, int nstages, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NWB_H */

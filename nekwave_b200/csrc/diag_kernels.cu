@@ -1,0 +1,87 @@
+// diag_kernels.cu -- device diagnostics: the FP64 discrete energy of
+// Case::computeTotalEnergy (src/case.cpp:733-766) as a deterministic two-pass
+// reduction, and an L2-evicting buffer write used between timed iterations.
+#include "nwb_internal.h"
+
+namespace nwb {
+namespace {
+
+constexpr int kEnergyThreads = 256;
+
+// Block b sums 1/2 (|E|^2 + |H|^2) J w3 over a contiguous range of nodes with a
+// fixed per-thread order and a fixed shuffle tree, so repeated calls agree bit
+// for bit.  jac_e (per element) or jac_n (per node) supplies J.
+__global__ void __launch_bounds__(kEnergyThreads)
+energy_partials_kernel(const double* __restrict__ u, long long stride, int N3,
+                       long long npts, const double* __restrict__ jac_e,
+                       const double* __restrict__ jac_n, const double* __restrict__ w3,
+                       double* __restrict__ partial) {
+    const long long per = (npts + gridDim.x - 1) / gridDim.x;
+    const long long lo = per * blockIdx.x;
+    const long long hi = min(npts, lo + per);
+    double acc = 0.0;
+    for (long long p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+        const long long e = p / N3;
+        const int m = static_cast<int>(p - e * N3);
+        const double J = jac_n ? jac_n[p] : jac_e[e];
+        const double dV = J * w3[m];
+        const double ex = u[p], ey = u[stride + p], ez = u[2 * stride + p];
+        const double hx = u[3 * stride + p], hy = u[4 * stride + p], hz = u[5 * stride + p];
+        const double eSq = ex * ex + ey * ey + ez * ez;
+        const double hSq = hx * hx + hy * hy + hz * hz;
+        acc += 0.5 * (eSq + hSq) * dV;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    __shared__ double warp_sums[kEnergyThreads / 32];
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kEnergyThreads / 32; ++w) s += warp_sums[w];
+        partial[blockIdx.x] = s;
+    }
+}
+
+__global__ void energy_final_kernel(const double* __restrict__ partial, int n,
+                                    double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < n; ++b) s += partial[b];
+        *out = s;
+    }
+}
+
+__global__ void l2_flush_kernel(int4* __restrict__ buf, size_t n16) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t x = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; x < n16; x += stride)
+        buf[x] = make_int4(static_cast<int>(x), 0, 0, 0);
+}
+
+}  // namespace
+
+int energy_blocks(int nelt) {
+    const int b = (nelt + 3) / 4;
+    return b < 1 ? 1 : (b > 1184 ? 1184 : b);
+}
+
+cudaError_t launch_energy(const double* u, long long stride, int N, int nelt,
+                          const double* jac_e, const double* jac_n, const double* w3,
+                          double* partial, int nblocks, double* out, cudaStream_t st) {
+    const int N3 = N * N * N;
+    const long long npts = static_cast<long long>(nelt) * N3;
+    energy_partials_kernel<<<nblocks, kEnergyThreads, 0, st>>>(u, stride, N3, npts, jac_e, jac_n,
+                                                               w3, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    energy_final_kernel<<<1, 32, 0, st>>>(partial, nblocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_l2_flush(void* buf, size_t bytes, cudaStream_t st) {
+    const size_t n16 = bytes / 16;
+    l2_flush_kernel<<<148 * 4, 256, 0, st>>>(static_cast<int4*>(buf), n16);
+    return cudaGetLastError();
+}
+
+}  // namespace nwb

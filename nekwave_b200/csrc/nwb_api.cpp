@@ -1,0 +1,616 @@
+// nwb_api.cpp -- host side of libnwb: the C ABI of include/nwb.h.
+//
+// nwb_solver replaces DgSolver::Impl (src/dg_solver.cpp:22-640).  At create time
+// the mesh arrays the reference uploads as-is are analysed once on the host and
+// compressed into the form the fused stage kernel streams:
+//   * affine elements (constant J^{-T} over the element, the case of every box
+//     mesh): one ElemGeo record per element (metrics, per-face normal and lift)
+//     plus one connection code per face -- O(nelt) geometry instead of the
+//     reference's 10 per-node and 7 per-face-point arrays;
+//   * anything else: per-node metrics and per-face-point normal/lift/neighbour
+//     arrays (the general path).
+// One stage is one kernel launch; a time step is five launches, optionally
+// replayed from a CUDA graph.
+#include "nwb.h"
+#include "nwb_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+nwb_status fail(nwb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define NWB_CU(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            return fail(e_ == cudaErrorMemoryAllocation ? NWB_ENOMEM : NWB_ECUDA,         \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                 \
+    } while (0)
+
+// Carpenter-Kennedy LSRK45 (src/dg_solver.cpp:58-69).
+const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                         -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kRK4B[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                         2277821191437.0 / 14882151754819.0};
+
+inline int face_local(int N, int f, int p, int q) {
+    switch (f) {
+        case 0: return p + N * N * q;
+        case 1: return (N - 1) + N * p + N * N * q;
+        case 2: return p + N * (N - 1) + N * N * q;
+        case 3: return N * p + N * N * q;
+        case 4: return p + N * q;
+        default: return p + N * q + N * N * (N - 1);
+    }
+}
+
+inline void orient(int N, int o, int p, int q, int* pp, int* qq) {
+    int a = (o & 4) ? q : p;
+    int b = (o & 4) ? p : q;
+    if (o & 1) a = N - 1 - a;
+    if (o & 2) b = N - 1 - b;
+    *pp = a;
+    *qq = b;
+}
+
+// Host-side result of the mesh analysis.
+struct Analysis {
+    int geo = nwb::GEO_NODAL;
+    std::vector<nwb::ElemGeo> egeo;
+    std::vector<int> conn;
+    std::vector<double> jac_e;
+};
+
+nwb_status analyse(const nwb_mesh_desc* m, Analysis* A) {
+    const int N = m->N, nelt = m->nelt, N2 = N * N, N3 = N2 * N;
+    const long long npts = static_cast<long long>(nelt) * N3;
+    // canonical face-point order (src/mesh.cpp:1003-1004) is part of the contract
+    for (int e = 0; e < nelt; ++e)
+        for (int f = 0; f < 6; ++f)
+            for (int pq = 0; pq < N2; ++pq) {
+                const long long fp = (static_cast<long long>(e) * 6 + f) * N2 + pq;
+                const int want = e * N3 + face_local(N, f, pq % N, pq / N);
+                if (m->vol_idx_minus[fp] != want)
+                    return fail(NWB_EINVAL,
+                                "face point %lld: vol_idx_minus %d, expected %d (face points must be "
+                                "element-major, faces 0..5, q, p)",
+                                fp, m->vol_idx_minus[fp], want);
+                const int vp = m->vol_idx_plus[fp];
+                if (vp >= npts)
+                    return fail(NWB_EINVAL, "face point %lld: vol_idx_plus %d out of range", fp, vp);
+            }
+    bool affine = true, box = true;
+    A->egeo.assign(nelt, nwb::ElemGeo{});
+    A->conn.assign(6 * static_cast<size_t>(nelt), nwb::kConnPEC);
+    A->jac_e.assign(nelt, 0.0);
+    for (int e = 0; e < nelt && affine; ++e) {
+        const long long base = static_cast<long long>(e) * N3;
+        nwb::ElemGeo& G = A->egeo[e];
+        double scale = 0.0;
+        for (int c = 0; c < 9; ++c) {
+            G.met[c] = m->met[c][base];
+            scale = std::max(scale, std::abs(G.met[c]));
+        }
+        const double J0 = m->jac[base];
+        G.jdet = J0;
+        A->jac_e[e] = J0;
+        for (int n = 0; n < N3 && affine; ++n) {
+            if (std::abs(m->jac[base + n] - J0) > 1e-12 * std::abs(J0)) affine = false;
+            for (int c = 0; c < 9; ++c)
+                if (std::abs(m->met[c][base + n] - G.met[c]) > 1e-12 * scale) affine = false;
+        }
+        for (int c : {1, 2, 3, 5, 6, 7})
+            if (std::abs(G.met[c]) > 1e-13 * scale) box = false;
+        for (int f = 0; f < 6 && affine; ++f) {
+            const long long fp0 = (static_cast<long long>(e) * 6 + f) * N2;
+            const bool pec0 = m->bc_type[fp0] != 0 || m->vol_idx_plus[fp0] < 0;
+            const double n0[3] = {m->nx[fp0], m->ny[fp0], m->nz[fp0]};
+            const int vm0 = m->vol_idx_minus[fp0];
+            const double lift0 = m->dA[fp0] / (m->jac[vm0] * m->w3[vm0 - base]);
+            for (int pq = 0; pq < N2; ++pq) {
+                const long long fp = fp0 + pq;
+                const bool pec = m->bc_type[fp] != 0 || m->vol_idx_plus[fp] < 0;
+                const int vm = m->vol_idx_minus[fp];
+                const double lift = m->dA[fp] / (m->jac[vm] * m->w3[vm - base]);
+                if (pec != pec0 || std::abs(m->nx[fp] - n0[0]) > 1e-12 ||
+                    std::abs(m->ny[fp] - n0[1]) > 1e-12 || std::abs(m->nz[fp] - n0[2]) > 1e-12 ||
+                    std::abs(lift - lift0) > 1e-12 * std::abs(lift0)) {
+                    affine = false;
+                    break;
+                }
+            }
+            if (!affine) break;
+            for (int c = 0; c < 3; ++c) G.nrm[f][c] = n0[c];
+            G.lift[f] = lift0;
+            if (pec0) {
+                A->conn[6 * static_cast<size_t>(e) + f] = nwb::kConnPEC;
+                continue;
+            }
+            const int eB = m->vol_idx_plus[fp0] / N3;
+            int found = -1;
+            for (int fB = 0; fB < 6 && found < 0; ++fB)
+                for (int o = 0; o < 8 && found < 0; ++o) {
+                    bool ok = true;
+                    for (int pq = 0; pq < N2 && ok; ++pq) {
+                        int a, b;
+                        orient(N, o, pq % N, pq / N, &a, &b);
+                        ok = m->vol_idx_plus[fp0 + pq] == eB * N3 + face_local(N, fB, a, b);
+                    }
+                    if (ok) found = (fB << 3) | o;
+                }
+            if (found < 0) { affine = false; break; }
+            A->conn[6 * static_cast<size_t>(e) + f] = (eB << 6) | found;
+        }
+    }
+    A->geo = !affine ? nwb::GEO_NODAL : (box ? nwb::GEO_BOX : nwb::GEO_AFFINE);
+    if (!affine) {
+        A->egeo.clear();
+        A->conn.clear();
+        A->jac_e.clear();
+    }
+    return NWB_OK;
+}
+
+template <class T>
+nwb_status dalloc(T** p, size_t count, size_t* total) {
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(NWB_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    *total += bytes;
+    return NWB_OK;
+}
+
+}  // namespace
+
+extern "C" void nwb_set_error_(const char* msg) { g_err = msg ? msg : ""; }
+
+struct nwb_solver {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    int N = 0, nelt = 0, geo = 0, f32 = 0;
+    long long npts = 0, stride = 0, nfp = 0;
+    double c0 = 1.0;
+    double* u[2] = {nullptr, nullptr};
+    double* k = nullptr;
+    int cur = 0;
+    double* dD = nullptr;
+    nwb::ElemGeo* dgeo = nullptr;
+    int* dconn = nullptr;
+    double* djac_e = nullptr;
+    double* dmet_n = nullptr;
+    double* dfnrm = nullptr;
+    double* dflift = nullptr;
+    int* dfplus = nullptr;
+    double* djac_n = nullptr;
+    double* dw3 = nullptr;
+    double* dpartial = nullptr;
+    double* denergy = nullptr;
+    int eblocks = 1;
+    void* dflush = nullptr;
+    size_t flush_bytes = 0;
+    nwb::StageConfig cfg{};
+    long long launches = 0;
+    size_t device_bytes = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    double gdt = 0.0;
+
+    nwb::StageParams params(int stage, double dt) const {
+        nwb::StageParams P{};
+        P.u_in = u[cur];
+        P.u_out = u[cur ^ 1];
+        P.k = k;
+        P.stride = stride;
+        P.nelt = nelt;
+        P.D = dD;
+        P.geo = dgeo;
+        P.conn = dconn;
+        P.met_n = dmet_n;
+        P.fnrm = dfnrm;
+        P.flift = dflift;
+        P.fplus = dfplus;
+        P.nfp = nfp;
+        P.c0 = c0;
+        P.a = kRK4A[stage];
+        P.b = kRK4B[stage];
+        P.dt = dt;
+        return P;
+    }
+
+    nwb_status launch_stage(int stage, double dt) {
+        nwb::StageParams P = params(stage, dt);
+        cudaError_t e = nwb::launch_stage(N, geo, f32, P, st, nullptr);
+        if (e != cudaSuccess) return fail(NWB_ECUDA, "stage kernel launch: %s", cudaGetErrorString(e));
+        cur ^= 1;
+        ++launches;
+        return NWB_OK;
+    }
+
+    nwb_status launch_step(double dt) {
+        for (int s = 0; s < 5; ++s) {
+            nwb_status r = launch_stage(s, dt);
+            if (r != NWB_OK) return r;
+        }
+        return NWB_OK;
+    }
+
+    void drop_graphs() {
+        for (auto& g : gexec)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+
+    // One-step graphs for both ping-pong parities, captured for this dt.
+    nwb_status ensure_graphs(double dt) {
+        if (gexec[0] && gexec[1] && gdt == dt) return NWB_OK;
+        drop_graphs();
+        const int cur0 = cur;
+        const long long l0 = launches;
+        for (int par = 0; par < 2; ++par) {
+            cur = par;
+            cudaGraph_t g = nullptr;
+            NWB_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            nwb_status r = launch_step(dt);
+            cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (r != NWB_OK) {
+                if (g) cudaGraphDestroy(g);
+                cur = cur0;
+                return r;
+            }
+            if (ce != cudaSuccess) {
+                cur = cur0;
+                return fail(NWB_ECUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ce));
+            }
+            ce = cudaGraphInstantiate(&gexec[par], g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) {
+                cur = cur0;
+                return fail(NWB_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ce));
+            }
+        }
+        cur = cur0;
+        launches = l0;
+        gdt = dt;
+        return NWB_OK;
+    }
+
+    nwb_status run_steps(double dt, int nsteps, bool graph) {
+        if (graph) {
+            nwb_status r = ensure_graphs(dt);
+            if (r != NWB_OK) return r;
+            for (int s = 0; s < nsteps; ++s) {
+                NWB_CU(cudaGraphLaunch(gexec[cur], st));
+                cur ^= 1;  // five stages: odd number of swaps
+                launches += 5;
+            }
+            return NWB_OK;
+        }
+        for (int s = 0; s < nsteps; ++s) {
+            nwb_status r = launch_step(dt);
+            if (r != NWB_OK) return r;
+        }
+        return NWB_OK;
+    }
+
+    void release() {
+        drop_graphs();
+        void* ptrs[] = {u[0], u[1], k, dD, dgeo, dconn, djac_e, dmet_n, dfnrm, dflift,
+                        dfplus, djac_n, dw3, dpartial, denergy, dflush};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+};
+
+extern "C" {
+
+const char* nwb_last_error(void) { return g_err.c_str(); }
+
+const char* nwb_status_string(nwb_status s) {
+    switch (s) {
+        case NWB_OK: return "NWB_OK";
+        case NWB_EINVAL: return "NWB_EINVAL";
+        case NWB_ENOMEM: return "NWB_ENOMEM";
+        case NWB_ECUDA: return "NWB_ECUDA";
+        case NWB_ETIMEOUT: return "NWB_ETIMEOUT";
+        case NWB_ENONFINITE: return "NWB_ENONFINITE";
+        case NWB_EBUSY: return "NWB_EBUSY";
+        case NWB_ENOTFOUND: return "NWB_ENOTFOUND";
+    }
+    return "NWB_UNKNOWN";
+}
+
+int nwb_version(void) { return NWB_VERSION; }
+
+nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision prec, nwb_solver** out) {
+    if (!out) return fail(NWB_EINVAL, "nwb_solver_create: out is null");
+    *out = nullptr;
+    if (!m) return fail(NWB_EINVAL, "nwb_solver_create: mesh is null");
+    if (m->N < 2 || m->N > 10) return fail(NWB_EINVAL, "nwb_solver_create: N=%d outside 2..10", m->N);
+    if (m->nelt < 1) return fail(NWB_EINVAL, "nwb_solver_create: nelt=%d", m->nelt);
+    if (prec != NWB_FP64 && prec != NWB_FP32_BULK)
+        return fail(NWB_EINVAL, "nwb_solver_create: unknown precision %d", static_cast<int>(prec));
+    if (!m->D || !m->w3 || !m->jac || !m->vol_idx_minus || !m->vol_idx_plus || !m->bc_type || !m->nx ||
+        !m->ny || !m->nz || !m->dA)
+        return fail(NWB_EINVAL, "nwb_solver_create: null mesh array");
+    for (int c = 0; c < 9; ++c)
+        if (!m->met[c]) return fail(NWB_EINVAL, "nwb_solver_create: null metric array %d", c);
+    if (!std::isfinite(c0)) return fail(NWB_EINVAL, "nwb_solver_create: c0 not finite");
+    const int N = m->N, N2 = N * N, N3 = N2 * N;
+    const long long npts = static_cast<long long>(m->nelt) * N3;
+    if (m->nelt > (1 << 25) || npts > 0x7fffffffLL)
+        return fail(NWB_EINVAL, "nwb_solver_create: mesh too large for 32-bit node indices");
+
+    Analysis A;
+    try {
+        nwb_status r = analyse(m, &A);
+        if (r != NWB_OK) return r;
+    } catch (const std::bad_alloc&) {
+        return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");
+    }
+
+    nwb_solver* s = new (std::nothrow) nwb_solver();
+    if (!s) return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");
+    auto bail = [&](nwb_status r) {
+        s->release();
+        delete s;
+        return r;
+    };
+    cudaError_t ce = cudaGetDevice(&s->device);
+    if (ce != cudaSuccess) {
+        delete s;
+        return fail(NWB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(ce));
+    }
+    s->N = N;
+    s->nelt = m->nelt;
+    s->npts = npts;
+    s->stride = (npts + 63) / 64 * 64;  // 512-byte aligned components
+    s->nfp = static_cast<long long>(m->nelt) * 6 * N2;
+    s->geo = A.geo;
+    s->f32 = prec == NWB_FP32_BULK ? 1 : 0;
+    s->c0 = c0;
+    s->eblocks = nwb::energy_blocks(m->nelt);
+    ce = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce)));
+
+    ce = nwb::stage_config(N, s->geo, s->f32, &s->cfg);
+    if (ce != cudaSuccess)
+        return bail(fail(NWB_ECUDA, "stage kernel set-up: %s", cudaGetErrorString(ce)));
+
+    size_t& tot = s->device_bytes;
+    nwb_status r = NWB_OK;
+#define NWB_TRY(x)                  \
+    do {                            \
+        r = (x);                    \
+        if (r != NWB_OK) return bail(r); \
+    } while (0)
+    NWB_TRY(dalloc(&s->u[0], 6 * static_cast<size_t>(s->stride), &tot));
+    NWB_TRY(dalloc(&s->u[1], 6 * static_cast<size_t>(s->stride), &tot));
+    NWB_TRY(dalloc(&s->k, 6 * static_cast<size_t>(s->stride), &tot));
+    NWB_TRY(dalloc(&s->dD, static_cast<size_t>(N2), &tot));
+    NWB_TRY(dalloc(&s->dw3, static_cast<size_t>(N3), &tot));
+    NWB_TRY(dalloc(&s->dpartial, static_cast<size_t>(s->eblocks), &tot));
+    NWB_TRY(dalloc(&s->denergy, 1, &tot));
+#define NWB_H2D(dst, src, bytes) \
+    do { ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
+         if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
+    NWB_H2D(s->dD, m->D, sizeof(double) * N2);
+    NWB_H2D(s->dw3, m->w3, sizeof(double) * N3);
+    if (s->geo != nwb::GEO_NODAL) {
+        NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(m->nelt), &tot));
+        NWB_TRY(dalloc(&s->dconn, 6 * static_cast<size_t>(m->nelt), &tot));
+        NWB_TRY(dalloc(&s->djac_e, static_cast<size_t>(m->nelt), &tot));
+        NWB_H2D(s->dgeo, A.egeo.data(), sizeof(nwb::ElemGeo) * m->nelt);
+        NWB_H2D(s->dconn, A.conn.data(), sizeof(int) * 6 * static_cast<size_t>(m->nelt));
+        NWB_H2D(s->djac_e, A.jac_e.data(), sizeof(double) * m->nelt);
+    } else {
+        const size_t nfp = static_cast<size_t>(s->nfp);
+        try {
+            std::vector<double> fn(3 * nfp), fl(nfp);
+            std::vector<int> fpl(nfp);
+            for (size_t fp = 0; fp < nfp; ++fp) {
+                const int vm = m->vol_idx_minus[fp];
+                const bool pec = m->bc_type[fp] != 0 || m->vol_idx_plus[fp] < 0;
+                fn[fp] = m->nx[fp];
+                fn[nfp + fp] = m->ny[fp];
+                fn[2 * nfp + fp] = m->nz[fp];
+                fl[fp] = m->dA[fp] / (m->jac[vm] * m->w3[vm % N3]);
+                fpl[fp] = pec ? -1 : m->vol_idx_plus[fp];
+            }
+            NWB_TRY(dalloc(&s->dmet_n, 9 * static_cast<size_t>(s->stride), &tot));
+            NWB_TRY(dalloc(&s->djac_n, static_cast<size_t>(npts), &tot));
+            NWB_TRY(dalloc(&s->dfnrm, 3 * nfp, &tot));
+            NWB_TRY(dalloc(&s->dflift, nfp, &tot));
+            NWB_TRY(dalloc(&s->dfplus, nfp, &tot));
+            for (int c = 0; c < 9; ++c) NWB_H2D(s->dmet_n + c * s->stride, m->met[c], sizeof(double) * npts);
+            NWB_H2D(s->djac_n, m->jac, sizeof(double) * npts);
+            NWB_H2D(s->dfnrm, fn.data(), sizeof(double) * 3 * nfp);
+            NWB_H2D(s->dflift, fl.data(), sizeof(double) * nfp);
+            NWB_H2D(s->dfplus, fpl.data(), sizeof(int) * nfp);
+        } catch (const std::bad_alloc&) {
+            return bail(fail(NWB_ENOMEM, "nwb_solver_create: out of host memory"));
+        }
+    }
+    // state and LSRK register start at zero (src/dg_solver.cpp:122-125)
+    for (int b = 0; b < 2; ++b) {
+        ce = cudaMemset(s->u[b], 0, sizeof(double) * 6 * s->stride);
+        if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "memset: %s", cudaGetErrorString(ce)));
+    }
+    ce = cudaMemset(s->k, 0, sizeof(double) * 6 * s->stride);
+    if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "memset: %s", cudaGetErrorString(ce)));
+    ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "set-up: %s", cudaGetErrorString(ce)));
+#undef NWB_TRY
+#undef NWB_H2D
+    *out = s;
+    return NWB_OK;
+}
+
+nwb_status nwb_upload_state(nwb_solver* s, const double* h, size_t n) {
+    if (!s || !h) return fail(NWB_EINVAL, "nwb_upload_state: null argument");
+    if (n != 6 * static_cast<size_t>(s->npts))
+        return fail(NWB_EINVAL, "nwb_upload_state: size %zu, expected 6*npts = %lld", n, 6 * s->npts);
+    NWB_CU(cudaMemcpy2DAsync(s->u[s->cur], sizeof(double) * s->stride, h, sizeof(double) * s->npts,
+                             sizeof(double) * s->npts, 6, cudaMemcpyHostToDevice, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_download_state(nwb_solver* s, double* h, size_t n) {
+    if (!s || !h) return fail(NWB_EINVAL, "nwb_download_state: null argument");
+    if (n != 6 * static_cast<size_t>(s->npts))
+        return fail(NWB_EINVAL, "nwb_download_state: size %zu, expected 6*npts = %lld", n, 6 * s->npts);
+    NWB_CU(cudaMemcpy2DAsync(h, sizeof(double) * s->npts, s->u[s->cur], sizeof(double) * s->stride,
+                             sizeof(double) * s->npts, 6, cudaMemcpyDeviceToHost, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_step(nwb_solver* s, double dt, int nsteps) {
+    if (!s) return fail(NWB_EINVAL, "nwb_step: null solver");
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(NWB_EINVAL, "nwb_step: bad dt/nsteps");
+    if (nsteps == 0) return NWB_OK;
+    return s->run_steps(dt, nsteps, nsteps > 1);
+}
+
+nwb_status nwb_sync(nwb_solver* s) {
+    if (!s) return fail(NWB_EINVAL, "nwb_sync: null solver");
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_eval_rhs(nwb_solver* s, double* h, size_t n) {
+    if (!s || !h) return fail(NWB_EINVAL, "nwb_eval_rhs: null argument");
+    if (n != 6 * static_cast<size_t>(s->npts))
+        return fail(NWB_EINVAL, "nwb_eval_rhs: size %zu, expected 6*npts", n);
+    // one stage with a = 0, b = 0, dt = 1 leaves k = rhs and copies u_in into the
+    // spare buffer; the state itself (u[cur]) is untouched
+    NWB_CU(cudaMemsetAsync(s->k, 0, sizeof(double) * 6 * s->stride, s->st));
+    nwb::StageParams P = s->params(0, 1.0);
+    P.a = 0.0;
+    P.b = 0.0;
+    cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, P, s->st, nullptr);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "stage kernel launch: %s", cudaGetErrorString(e));
+    ++s->launches;
+    NWB_CU(cudaMemcpy2DAsync(h, sizeof(double) * s->npts, s->k, sizeof(double) * s->stride,
+                             sizeof(double) * s->npts, 6, cudaMemcpyDeviceToHost, s->st));
+    NWB_CU(cudaMemsetAsync(s->k, 0, sizeof(double) * 6 * s->stride, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_energy(nwb_solver* s, double* out) {
+    if (!s || !out) return fail(NWB_EINVAL, "nwb_energy: null argument");
+    cudaError_t e = nwb::launch_energy(s->u[s->cur], s->stride, s->N, s->nelt, s->djac_e, s->djac_n,
+                                       s->dw3, s->dpartial, s->eblocks, s->denergy, s->st);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "energy kernel: %s", cudaGetErrorString(e));
+    s->launches += 2;
+    NWB_CU(cudaMemcpyAsync(out, s->denergy, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    if (!std::isfinite(*out)) return fail(NWB_ENONFINITE, "nwb_energy: state holds NaN/Inf");
+    return NWB_OK;
+}
+
+nwb_status nwb_solver_destroy(nwb_solver* s) {
+    if (!s) return NWB_OK;
+    cudaStreamSynchronize(s->st);
+    s->release();
+    delete s;
+    return NWB_OK;
+}
+
+nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info) {
+    if (!s || !info) return fail(NWB_EINVAL, "nwb_solver_get_info: null argument");
+    info->N = s->N;
+    info->nelt = s->nelt;
+    info->npts = s->npts;
+    info->stride = s->stride;
+    info->geometry = s->geo;
+    info->precision = s->f32;
+    info->ks = s->cfg.ks;
+    info->epb = s->cfg.epb;
+    info->threads_per_block = s->cfg.threads;
+    info->smem_bytes = s->cfg.smem;
+    info->device_bytes = static_cast<long long>(s->device_bytes);
+    return NWB_OK;
+}
+
+nwb_status nwb_solver_device_state(nwb_solver* s, double** d_state, void** stream) {
+    if (!s) return fail(NWB_EINVAL, "nwb_solver_device_state: null solver");
+    if (d_state) *d_state = s->u[s->cur];
+    if (stream) *stream = s->st;
+    return NWB_OK;
+}
+
+nwb_status nwb_solver_launch_count(const nwb_solver* s, long long* count) {
+    if (!s || !count) return fail(NWB_EINVAL, "nwb_solver_launch_count: null argument");
+    *count = s->launches;
+    return NWB_OK;
+}
+
+nwb_status nwb_time_steps(nwb_solver* s, double dt, int nsteps, int use_graph, float* ms) {
+    if (!s || !ms || nsteps < 1) return fail(NWB_EINVAL, "nwb_time_steps: bad argument");
+    if (use_graph) {
+        nwb_status r = s->ensure_graphs(dt);
+        if (r != NWB_OK) return r;
+    }
+    cudaEvent_t a, b;
+    NWB_CU(cudaEventCreate(&a));
+    NWB_CU(cudaEventCreate(&b));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    NWB_CU(cudaEventRecord(a, s->st));
+    nwb_status r = s->run_steps(dt, nsteps, use_graph != 0);
+    NWB_CU(cudaEventRecord(b, s->st));
+    NWB_CU(cudaEventSynchronize(b));
+    NWB_CU(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return r;
+}
+
+nwb_status nwb_time_stage_kernel(nwb_solver* s, double dt, int nstages, float* ms) {
+    if (!s || !ms || nstages < 1) return fail(NWB_EINVAL, "nwb_time_stage_kernel: bad argument");
+    cudaEvent_t a, b;
+    NWB_CU(cudaEventCreate(&a));
+    NWB_CU(cudaEventCreate(&b));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    NWB_CU(cudaEventRecord(a, s->st));
+    nwb_status r = NWB_OK;
+    for (int i = 0; i < nstages && r == NWB_OK; ++i) r = s->launch_stage(i % 5, dt);
+    NWB_CU(cudaEventRecord(b, s->st));
+    NWB_CU(cudaEventSynchronize(b));
+    float t = 0.f;
+    NWB_CU(cudaEventElapsedTime(&t, a, b));
+    *ms = t / nstages;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return r;
+}
+
+}  // extern "C"

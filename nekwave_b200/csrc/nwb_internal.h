@@ -1,0 +1,81 @@
+// nwb_internal.h -- types shared by the host side (nwb_api.cpp) and the CUDA
+// kernels (stage_kernels.cu, diag_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nwb {
+
+// Geometry classes the mesh analysis sorts a mesh into (nwb_api.cpp).
+enum GeoKind : int {
+    GEO_BOX = 0,     // affine, axis-aligned: metrics diag(rx, sy, tz) per element
+    GEO_AFFINE = 1,  // affine: full constant J^{-T} per element
+    GEO_NODAL = 2    // per-node metrics and per-face-point normals/lift/neighbours
+};
+
+// Per-element geometry for the affine classes.  The reference weights the volume
+// curl by w3*J (src/device/dg_kernels.cu:127) and divides by J*w3 again in the
+// inverse-mass kernel (:369-370); the two cancel, so only J^{-T} remains.  The
+// lift of face f is dA/(J w3) at its nodes, which for an affine element is the
+// constant |J J^{-T} n_ref| / (J w_end) (src/mesh.cpp:1011-1038).
+struct alignas(16) ElemGeo {
+    double met[9];      // rx sx tx ry sy ty rz sz tz
+    double nrm[6][3];   // outward unit normal of face f
+    double lift[6];     // dA/(J w3) at the nodes of face f
+    double jdet;        // J (energy weight); 34 doubles = 272 bytes
+};
+static_assert(sizeof(ElemGeo) == 272, "ElemGeo layout");
+
+// Face connection code of (element, face):
+//   -1                          PEC mirror ([[E]] = -2E^-, [[H]] = 0)
+//   (eB << 6) | (fB << 3) | o   neighbour element eB, its face fB, orientation o
+// Orientation o maps (p,q) on this face to (p',q') on the neighbour face:
+//   (a,b) = (o & 4) ? (q,p) : (p,q);  p' = (o & 1) ? N-1-a : a;  q' = (o & 2) ? N-1-b : b.
+constexpr int kConnPEC = -1;
+
+struct StageParams {
+    const double* u_in;     // [6][stride]
+    double* u_out;          // [6][stride]
+    double* k;              // [6][stride], updated in place
+    long long stride;       // component stride (doubles)
+    int nelt;
+    int _pad0;
+    const double* D;        // [N*N] column-major
+    const ElemGeo* geo;     // [nelt]       (GEO_BOX, GEO_AFFINE)
+    const int* conn;        // [nelt*6]     (GEO_BOX, GEO_AFFINE)
+    const double* met_n;    // [9][stride]  (GEO_NODAL)
+    const double* fnrm;     // [3][nfp]     (GEO_NODAL)
+    const double* flift;    // [nfp]        (GEO_NODAL)
+    const int* fplus;       // [nfp] neighbour node, -1 mirror (GEO_NODAL)
+    long long nfp;
+    double c0;              // flux penalty: 0 central, 1 upwind
+    double a, b, dt;        // LSRK45 stage coefficients and step
+};
+
+// Launch configuration of the fused stage kernel for one N.
+struct StageConfig {
+    int ks;       // threads per (i,j) node column
+    int epb;      // elements per block
+    int threads;  // threads per block
+    int smem;     // dynamic shared memory bytes
+};
+
+// Fused stage kernel launcher (stage_kernels.cu).  Returns cudaErrorInvalidValue
+// when N/geo/precision has no instantiation.
+cudaError_t launch_stage(int N, int geo, int f32, const StageParams& p, cudaStream_t st,
+                         StageConfig* cfg_out);
+cudaError_t stage_config(int N, int geo, int f32, StageConfig* cfg);
+
+// FP64 energy of the state u (diag_kernels.cu): nblocks partial sums, then one
+// fixed-order final sum into *out (device).  J comes from jac_e (per element,
+// affine meshes) or jac_n (per node).
+cudaError_t launch_energy(const double* u, long long stride, int N, int nelt,
+                          const double* jac_e, const double* jac_n, const double* w3,
+                          double* partial, int nblocks, double* out, cudaStream_t st);
+int energy_blocks(int nelt);
+
+// Large buffer write that evicts L2 (benchmark hygiene).
+cudaError_t launch_l2_flush(void* buf, size_t bytes, cudaStream_t st);
+
+}  // namespace nwb

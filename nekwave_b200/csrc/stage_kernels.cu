@@ -1,0 +1,448 @@
+// stage_kernels.cu -- the fused LSRK45 stage kernel for sm_100a.
+//
+// One launch performs, for every element, everything the reference does in
+// seven launches per stage (src/dg_solver.cpp:393-505):
+//   volume curl of H and E        (src/device/dg_kernels.cu:41-155, twice)
+//   face traces, numerical flux   (:170-304; PEC mirror and neighbour traces)
+//   surface lift and inverse mass (:316-382, without atomics)
+//   LSRK45 update                 (:393-408)
+// The state is ping-ponged (u_in -> u_out) because neighbour traces of u_in are
+// read while other blocks write their updated elements; k is updated in place.
+//
+// Block = EPB elements; each element is handled by a team of KS*N*N threads,
+// thread (i,j,h) owning node column (i,j) for the planes k of its share h.
+// Per block:
+//   1. cp.async stages u_in and k of the EPB elements in shared memory
+//      (two commit groups, so k arrives while the flux and volume work runs);
+//   2. face phase: one thread per face point computes the numerical flux from
+//      its own trace (shared memory) and the neighbour trace (shared memory if
+//      the neighbour is in the same block, else global/L2), multiplies it by the
+//      FP64 lift dA/(J w3) and stores it in shared memory;
+//   3. column phase: GLL sum-factorised derivatives from shared memory, the
+//      physical curl, the lifted face terms of the faces the node lies on, the
+//      LSRK update in FP64, and coalesced stores of k and u_out.
+// Each residual entry is formed once by one thread in a fixed order: the
+// kernel is deterministic (the reference's atomic lift is not).
+#include "nwb_internal.h"
+
+#include <type_traits>
+
+namespace nwb {
+namespace {
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
+}
+
+// Local node of face point (p,q) on face f: Mesh::getFaceNodeVolIndex without
+// the element offset (src/mesh.cpp:955-981).
+template <int N>
+__device__ __forceinline__ int face_local(int f, int p, int q) {
+    switch (f) {
+        case 0: return p + N * N * q;                      // s = -1: i=p, j=0,   k=q
+        case 1: return (N - 1) + N * p + N * N * q;        // r = +1: i=N-1, j=p, k=q
+        case 2: return p + N * (N - 1) + N * N * q;        // s = +1: i=p, j=N-1, k=q
+        case 3: return N * p + N * N * q;                  // r = -1: i=0,   j=p, k=q
+        case 4: return p + N * q;                          // t = -1: i=p, j=q,   k=0
+        default: return p + N * q + N * N * (N - 1);       // t = +1: i=p, j=q,   k=N-1
+    }
+}
+
+constexpr int align16(int b) { return (b + 15) & ~15; }
+
+template <int N, bool F32, int EPB>
+struct SmemLayout {
+    static constexpr int N2 = N * N, N3 = N2 * N;
+    static constexpr int u = 0;
+    static constexpr int k = u + EPB * 6 * N3 * 8;
+    static constexpr int D = k + EPB * 6 * N3 * 8;
+    static constexpr int geo = D + align16(N2 * 8);
+    static constexpr int conn = geo + EPB * static_cast<int>(sizeof(ElemGeo));
+    static constexpr int flux = conn + align16(EPB * 6 * 4);
+    static constexpr int uc = flux + EPB * 36 * N2 * 8;
+    static constexpr int total = uc + (F32 ? EPB * 6 * N3 * 4 : 0);
+};
+
+// Numerical flux of src/device/dg_kernels.cu:264-294 for jumps dE = E+ - E-,
+// dH = H+ - H-: fH = -1/2 n x[[E]] - c0/2 n x(n x[[H]]), fE = +1/2 n x[[H]] - c0/2 n x(n x[[E]]).
+template <typename T>
+__device__ __forceinline__ void numerical_flux(T nx, T ny, T nz, T hc0, T dEx, T dEy, T dEz,
+                                               T dHx, T dHy, T dHz, T f[6]) {
+    const T nxE_x = ny * dEz - nz * dEy;
+    const T nxE_y = nz * dEx - nx * dEz;
+    const T nxE_z = nx * dEy - ny * dEx;
+    const T nxH_x = ny * dHz - nz * dHy;
+    const T nxH_y = nz * dHx - nx * dHz;
+    const T nxH_z = nx * dHy - ny * dHx;
+    const T nnE_x = ny * nxE_z - nz * nxE_y;
+    const T nnE_y = nz * nxE_x - nx * nxE_z;
+    const T nnE_z = nx * nxE_y - ny * nxE_x;
+    const T nnH_x = ny * nxH_z - nz * nxH_y;
+    const T nnH_y = nz * nxH_x - nx * nxH_z;
+    const T nnH_z = nx * nxH_y - ny * nxH_x;
+    const T half = T(0.5);
+    // residual order: E components first, then H (the reference lifts flux[3..5]
+    // into resE and flux[0..2] into resH, src/device/dg_kernels.cu:329-336)
+    f[0] = half * nxH_x - hc0 * nnE_x;
+    f[1] = half * nxH_y - hc0 * nnE_y;
+    f[2] = half * nxH_z - hc0 * nnE_z;
+    f[3] = -half * nxE_x - hc0 * nnH_x;
+    f[4] = -half * nxE_y - hc0 * nnH_y;
+    f[5] = -half * nxE_z - hc0 * nnH_z;
+}
+
+template <int N, int GEO, bool F32, int KS, int EPB>
+__global__ void __launch_bounds__(EPB * KS * N * N)
+    stage_kernel(const StageParams P) {
+    using TC = typename std::conditional<F32, float, double>::type;
+    constexpr int N2 = N * N, N3 = N2 * N;
+    constexpr int TPE = KS * N2;          // threads per element
+    constexpr int NT = EPB * TPE;         // threads per block
+    constexpr int KPT = (N + KS - 1) / KS;
+    constexpr int CS = EPB * N3;          // component stride in shared memory
+    using L = SmemLayout<N, F32, EPB>;
+
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* s_u = reinterpret_cast<double*>(smem + L::u);
+    double* s_k = reinterpret_cast<double*>(smem + L::k);
+    double* s_D = reinterpret_cast<double*>(smem + L::D);
+    ElemGeo* s_geo = reinterpret_cast<ElemGeo*>(smem + L::geo);
+    int* s_conn = reinterpret_cast<int*>(smem + L::conn);
+    double* s_flux = reinterpret_cast<double*>(smem + L::flux);
+    TC* s_uc;
+    if constexpr (F32) s_uc = reinterpret_cast<TC*>(smem + L::uc);
+    else s_uc = reinterpret_cast<TC*>(s_u);
+
+    const int tid = threadIdx.x;
+    const int team = tid / TPE;
+    const int lt = tid - team * TPE;
+    const int loc = lt % N2;
+    const int h = lt / N2;
+    const int i = loc % N;
+    const int j = loc / N;
+    const int e0 = blockIdx.x * EPB;
+    const int nvalid = min(EPB, P.nelt - e0);
+    const int e = e0 + team;
+    const bool active = team < nvalid;
+    const long long S = P.stride;
+
+    // ---- 1. stage u_in (+ D, geometry) then k in shared memory ---------------
+    {
+        const long long gbase = static_cast<long long>(e0) * N3;
+        const int cnt = nvalid * N3;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double* src = P.u_in + c * S + gbase;
+            for (int x = tid; x < cnt; x += NT) cp_async8(s_u + c * CS + x, src + x);
+        }
+        for (int x = tid; x < N2; x += NT) cp_async8(s_D + x, P.D + x);
+        if constexpr (GEO != GEO_NODAL) {
+            const double* gsrc = reinterpret_cast<const double*>(P.geo + e0);
+            double* gdst = reinterpret_cast<double*>(s_geo);
+            const int gcnt = nvalid * static_cast<int>(sizeof(ElemGeo) / 8);
+            for (int x = tid; x < gcnt; x += NT) cp_async8(gdst + x, gsrc + x);
+            for (int x = tid; x < nvalid * 6; x += NT) s_conn[x] = P.conn[e0 * 6 + x];
+        }
+        cp_async_commit();
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double* src = P.k + c * S + gbase;
+            for (int x = tid; x < cnt; x += NT) cp_async8(s_k + c * CS + x, src + x);
+        }
+        cp_async_commit();
+    }
+    cp_async_wait<1>();
+    __syncthreads();
+    if constexpr (F32) {
+        const int cnt = nvalid * N3;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            for (int x = tid; x < cnt; x += NT) s_uc[c * CS + x] = static_cast<float>(s_u[c * CS + x]);
+        __syncthreads();
+    }
+
+    // ---- 2. face phase: lifted numerical flux per face point -----------------
+    if (active) {
+        const TC* U = s_uc + team * N3;
+        for (int fp = lt; fp < 6 * N2; fp += TPE) {
+            const int f = fp / N2;
+            const int pq = fp - f * N2;
+            const int p = pq % N, q = pq / N;
+            const int m = face_local<N>(f, p, q);
+            const TC Exm = U[0 * CS + m], Eym = U[1 * CS + m], Ezm = U[2 * CS + m];
+            const TC Hxm = U[3 * CS + m], Hym = U[4 * CS + m], Hzm = U[5 * CS + m];
+            long long vB = -1;  // neighbour node (global index), -1 = mirror
+            double nxd, nyd, nzd, lift;
+            if constexpr (GEO == GEO_NODAL) {
+                const long long g = (static_cast<long long>(e) * 6 + f) * N2 + pq;
+                vB = P.fplus[g];
+                nxd = P.fnrm[g];
+                nyd = P.fnrm[P.nfp + g];
+                nzd = P.fnrm[2 * P.nfp + g];
+                lift = P.flift[g];
+            } else {
+                const int cd = s_conn[team * 6 + f];
+                if (cd != kConnPEC) {
+                    const int eB = cd >> 6, fB = (cd >> 3) & 7, o = cd & 7;
+                    int a = (o & 4) ? q : p;
+                    int b = (o & 4) ? p : q;
+                    if (o & 1) a = N - 1 - a;
+                    if (o & 2) b = N - 1 - b;
+                    vB = static_cast<long long>(eB) * N3 + face_local<N>(fB, a, b);
+                }
+                const ElemGeo& G = s_geo[team];
+                nxd = G.nrm[f][0];
+                nyd = G.nrm[f][1];
+                nzd = G.nrm[f][2];
+                lift = G.lift[f];
+            }
+            TC dEx, dEy, dEz, dHx, dHy, dHz;
+            if (vB < 0) {
+                // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
+                dEx = TC(-2) * Exm; dEy = TC(-2) * Eym; dEz = TC(-2) * Ezm;
+                dHx = TC(0); dHy = TC(0); dHz = TC(0);
+            } else {
+                const long long eB = vB / N3;
+                TC vals[6];
+                if (eB >= e0 && eB < e0 + nvalid) {
+                    const int sidx = static_cast<int>(vB - static_cast<long long>(e0) * N3);
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) vals[c] = s_uc[c * CS + sidx];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) vals[c] = static_cast<TC>(__ldg(P.u_in + c * S + vB));
+                }
+                dEx = vals[0] - Exm; dEy = vals[1] - Eym; dEz = vals[2] - Ezm;
+                dHx = vals[3] - Hxm; dHy = vals[4] - Hym; dHz = vals[5] - Hzm;
+            }
+            TC fl[6];
+            numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
+                               static_cast<TC>(0.5 * P.c0), dEx, dEy, dEz, dHx, dHy, dHz, fl);
+            double* F = s_flux + (team * 6 + f) * 6 * N2 + pq;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+
+    // ---- 3. column phase: volume curl + face terms + LSRK update --------------
+    if (!active) return;
+    const TC* U = s_uc + team * N3;
+    const double* Fl = s_flux + team * 36 * N2;
+    TC Dr[N], Ds[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        Dr[l] = static_cast<TC>(s_D[i + l * N]);
+        Ds[l] = static_cast<TC>(s_D[j + l * N]);
+    }
+    TC m_[9];
+    if constexpr (GEO != GEO_NODAL) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) m_[c] = static_cast<TC>(s_geo[team].met[c]);
+    }
+    const double A = P.a, B = P.b, DT = P.dt;
+    const long long ebase = static_cast<long long>(e) * N3;
+
+#pragma unroll
+    for (int kk = 0; kk < KPT; ++kk) {
+        const int k = h * KPT + kk;
+        if (KS > 1 && k >= N) break;
+        const int mloc = i + N * j + N2 * k;
+        double rhs[6];
+        if constexpr (GEO == GEO_BOX) {
+            // only the six derivatives a curl needs when J^{-T} = diag(rx, sy, tz)
+            TC Hz_r = 0, Hy_r = 0, Ez_r = 0, Ey_r = 0;
+            TC Hz_s = 0, Hx_s = 0, Ez_s = 0, Ex_s = 0;
+            TC Hy_t = 0, Hx_t = 0, Ey_t = 0, Ex_t = 0;
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                const TC dr = Dr[l], ds = Ds[l];
+                const TC dt = static_cast<TC>(s_D[k + l * N]);
+                const int ir = N2 * k + N * j + l;
+                const int is = N2 * k + N * l + i;
+                const int it = N2 * l + N * j + i;
+                Hz_r += dr * U[5 * CS + ir]; Hy_r += dr * U[4 * CS + ir];
+                Ez_r += dr * U[2 * CS + ir]; Ey_r += dr * U[1 * CS + ir];
+                Hz_s += ds * U[5 * CS + is]; Hx_s += ds * U[3 * CS + is];
+                Ez_s += ds * U[2 * CS + is]; Ex_s += ds * U[0 * CS + is];
+                Hy_t += dt * U[4 * CS + it]; Hx_t += dt * U[3 * CS + it];
+                Ey_t += dt * U[1 * CS + it]; Ex_t += dt * U[0 * CS + it];
+            }
+            const TC rx = m_[0], sy = m_[4], tz = m_[8];
+            rhs[0] = static_cast<double>(sy * Hz_s - tz * Hy_t);
+            rhs[1] = static_cast<double>(tz * Hx_t - rx * Hz_r);
+            rhs[2] = static_cast<double>(rx * Hy_r - sy * Hx_s);
+            rhs[3] = static_cast<double>(tz * Ey_t - sy * Ez_s);
+            rhs[4] = static_cast<double>(rx * Ez_r - tz * Ex_t);
+            rhs[5] = static_cast<double>(sy * Ex_s - rx * Ey_r);
+        } else {
+            TC dr_[6] = {0, 0, 0, 0, 0, 0}, ds_[6] = {0, 0, 0, 0, 0, 0}, dt_[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                const TC dr = Dr[l], ds = Ds[l];
+                const TC dt = static_cast<TC>(s_D[k + l * N]);
+                const int ir = N2 * k + N * j + l;
+                const int is = N2 * k + N * l + i;
+                const int it = N2 * l + N * j + i;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    dr_[c] += dr * U[c * CS + ir];
+                    ds_[c] += ds * U[c * CS + is];
+                    dt_[c] += dt * U[c * CS + it];
+                }
+            }
+            TC rx, sx, tx, ry, sy, ty, rz, sz, tz;
+            if constexpr (GEO == GEO_NODAL) {
+                const long long g = ebase + mloc;
+                rx = static_cast<TC>(P.met_n[0 * S + g]); sx = static_cast<TC>(P.met_n[1 * S + g]);
+                tx = static_cast<TC>(P.met_n[2 * S + g]); ry = static_cast<TC>(P.met_n[3 * S + g]);
+                sy = static_cast<TC>(P.met_n[4 * S + g]); ty = static_cast<TC>(P.met_n[5 * S + g]);
+                rz = static_cast<TC>(P.met_n[6 * S + g]); sz = static_cast<TC>(P.met_n[7 * S + g]);
+                tz = static_cast<TC>(P.met_n[8 * S + g]);
+            } else {
+                rx = m_[0]; sx = m_[1]; tx = m_[2]; ry = m_[3]; sy = m_[4];
+                ty = m_[5]; rz = m_[6]; sz = m_[7]; tz = m_[8];
+            }
+            // physical curl, src/device/dg_kernels.cu:140-149; E residual = +curl H,
+            // H residual = -curl E
+#pragma unroll
+            for (int fld = 0; fld < 2; ++fld) {
+                const int o = fld == 0 ? 3 : 0;
+                const TC u1r = dr_[o], u1s = ds_[o], u1t = dt_[o];
+                const TC u2r = dr_[o + 1], u2s = ds_[o + 1], u2t = dt_[o + 1];
+                const TC u3r = dr_[o + 2], u3s = ds_[o + 2], u3t = dt_[o + 2];
+                const TC c1 = (u3r * ry + u3s * sy + u3t * ty) - (u2r * rz + u2s * sz + u2t * tz);
+                const TC c2 = (u1r * rz + u1s * sz + u1t * tz) - (u3r * rx + u3s * sx + u3t * tx);
+                const TC c3 = (u2r * rx + u2s * sx + u2t * tx) - (u1r * ry + u1s * sy + u1t * ty);
+                const double sg = fld == 0 ? 1.0 : -1.0;
+                rhs[3 * fld + 0] = sg * static_cast<double>(c1);
+                rhs[3 * fld + 1] = sg * static_cast<double>(c2);
+                rhs[3 * fld + 2] = sg * static_cast<double>(c3);
+            }
+        }
+        // lifted face terms, faces in the reference's order 0..5
+        if (j == 0) {
+            const double* F = Fl + 0 * 6 * N2 + (i + N * k);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        if (i == N - 1) {
+            const double* F = Fl + 1 * 6 * N2 + (j + N * k);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        if (j == N - 1) {
+            const double* F = Fl + 2 * 6 * N2 + (i + N * k);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        if (i == 0) {
+            const double* F = Fl + 3 * 6 * N2 + (j + N * k);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        if (k == 0) {
+            const double* F = Fl + 4 * 6 * N2 + (i + N * j);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        if (k == N - 1) {
+            const double* F = Fl + 5 * 6 * N2 + (i + N * j);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) rhs[c] += F[c * N2];
+        }
+        // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
+        const int sl = team * N3 + mloc;
+        const long long g = ebase + mloc;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double kn = A * s_k[c * CS + sl] + DT * rhs[c];
+            P.k[c * S + g] = kn;
+            P.u_out[c * S + g] = s_u[c * CS + sl] + B * kn;
+        }
+    }
+}
+
+// Per-N launch shape: threads per column (KS) and elements per block (EPB).
+template <int N> struct Shape;
+template <> struct Shape<2> { static constexpr int KS = 2, EPB = 16; };
+template <> struct Shape<3> { static constexpr int KS = 3, EPB = 8; };
+template <> struct Shape<4> { static constexpr int KS = 2, EPB = 4; };
+template <> struct Shape<5> { static constexpr int KS = 1, EPB = 4; };
+template <> struct Shape<6> { static constexpr int KS = 2, EPB = 2; };
+template <> struct Shape<7> { static constexpr int KS = 1, EPB = 2; };
+template <> struct Shape<8> { static constexpr int KS = 2, EPB = 1; };
+template <> struct Shape<9> { static constexpr int KS = 1, EPB = 1; };
+template <> struct Shape<10> { static constexpr int KS = 1, EPB = 1; };
+
+template <int N, int GEO, bool F32>
+cudaError_t launch_n(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
+    constexpr int KS = Shape<N>::KS, EPB = Shape<N>::EPB;
+    constexpr int threads = EPB * KS * N * N;
+    constexpr int smem = SmemLayout<N, F32, EPB>::total;
+    auto kern = stage_kernel<N, GEO, F32, KS, EPB>;
+    if (cfg) *cfg = StageConfig{KS, EPB, threads, smem};
+    // The opt-in shared-memory size is set on the first call, which the solver
+    // makes at creation (outside any stream capture).
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (!p) return cudaSuccess;
+    const int blocks = (p->nelt + EPB - 1) / EPB;
+    kern<<<blocks, threads, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t dispatch_geo(int geo, int f32, const StageParams* p, cudaStream_t st, StageConfig* c) {
+    switch (geo) {
+        case GEO_BOX:
+            return f32 ? launch_n<N, GEO_BOX, true>(p, st, c) : launch_n<N, GEO_BOX, false>(p, st, c);
+        case GEO_AFFINE:
+            return f32 ? launch_n<N, GEO_AFFINE, true>(p, st, c) : launch_n<N, GEO_AFFINE, false>(p, st, c);
+        case GEO_NODAL:
+            return f32 ? launch_n<N, GEO_NODAL, true>(p, st, c) : launch_n<N, GEO_NODAL, false>(p, st, c);
+        default:
+            return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t dispatch(int N, int geo, int f32, const StageParams* p, cudaStream_t st, StageConfig* c) {
+    switch (N) {
+        case 2: return dispatch_geo<2>(geo, f32, p, st, c);
+        case 3: return dispatch_geo<3>(geo, f32, p, st, c);
+        case 4: return dispatch_geo<4>(geo, f32, p, st, c);
+        case 5: return dispatch_geo<5>(geo, f32, p, st, c);
+        case 6: return dispatch_geo<6>(geo, f32, p, st, c);
+        case 7: return dispatch_geo<7>(geo, f32, p, st, c);
+        case 8: return dispatch_geo<8>(geo, f32, p, st, c);
+        case 9: return dispatch_geo<9>(geo, f32, p, st, c);
+        case 10: return dispatch_geo<10>(geo, f32, p, st, c);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_stage(int N, int geo, int f32, const StageParams& p, cudaStream_t st,
+                         StageConfig* cfg_out) {
+    return dispatch(N, geo, f32, &p, st, cfg_out);
+}
+
+cudaError_t stage_config(int N, int geo, int f32, StageConfig* cfg) {
+    return dispatch(N, geo, f32, nullptr, nullptr, cfg);
+}
+
+}  // namespace nwb

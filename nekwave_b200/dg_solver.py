@@ -1,0 +1,145 @@
+"""DgSolver: the reference's solver interface (src/dg_solver.hpp:35-102) on libnwb.
+
+    solver = DgSolver()
+    solver.initialize(mesh, c0)           # DgSolver::initialize
+    solver.uploadState(state, state.size) # DgSolver::uploadState
+    solver.step(dt, t)                    # DgSolver::step (blocking, one step)
+    solver.downloadState(state, state.size)
+    solver.finalize()
+
+Everything runs through the C ABI of include/nwb.h; there is no host fallback.
+Beyond the reference interface it exposes ``steps`` (many steps, asynchronous),
+``evalRhs`` and ``energy`` (device FP64 diagnostics).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import NWB_FP32_BULK, NWB_FP64, SolverInfo, check, dptr
+
+StateVector = np.ndarray  # [Ex, Ey, Ez, Hx, Hy, Hz], each of length npts (src/dg_solver.hpp:14)
+
+PRECISIONS = {"fp64": NWB_FP64, "fp32": NWB_FP32_BULK, "fp32_bulk": NWB_FP32_BULK}
+
+
+class DgSolver:
+    """GPU-resident DG-SEM Maxwell solver (src/dg_solver.hpp:35)."""
+
+    def __init__(self, precision: str = "fp64"):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self._prec = PRECISIONS[precision]
+        self._h = None
+        self._npts = 0
+
+    def initialize(self, mesh, c0: float) -> bool:
+        """Analyse the mesh and allocate the device state (DgSolver::initialize)."""
+        self.finalize()
+        L = _lib.lib()
+        h = C.c_void_p()
+        d = mesh.desc()
+        check(L.nwb_solver_create(C.byref(d), float(c0), self._prec, C.byref(h)))
+        self._h = h
+        self._npts = mesh.getTotalPoints()
+        self._mesh = mesh
+        return True
+
+    def _need(self):
+        if self._h is None:
+            raise RuntimeError("DgSolver not initialized")
+        return self._h
+
+    def uploadState(self, hostState: np.ndarray, size: int | None = None) -> None:
+        h = self._need()
+        a = np.ascontiguousarray(hostState, dtype=np.float64)
+        n = a.size if size is None else int(size)
+        if n > a.size:
+            raise ValueError("size larger than the host buffer")
+        check(_lib.lib().nwb_upload_state(h, dptr(a), n))
+
+    def downloadState(self, hostState: np.ndarray | None = None, size: int | None = None):
+        h = self._need()
+        out = np.empty(6 * self._npts) if hostState is None else hostState
+        if out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("host buffer must be a contiguous float64 array")
+        n = out.size if size is None else int(size)
+        if n > out.size:
+            raise ValueError("size larger than the host buffer")
+        check(_lib.lib().nwb_download_state(h, dptr(out), n))
+        return out
+
+    def step(self, dt: float, time: float = 0.0) -> None:
+        """One LSRK45 step; returns when it has finished, as the reference does."""
+        h = self._need()
+        L = _lib.lib()
+        check(L.nwb_step(h, float(dt), 1))
+        check(L.nwb_sync(h))
+
+    def steps(self, dt: float, nsteps: int, sync: bool = True) -> None:
+        """nsteps LSRK45 steps, replayed from a CUDA graph."""
+        h = self._need()
+        L = _lib.lib()
+        check(L.nwb_step(h, float(dt), int(nsteps)))
+        if sync:
+            check(L.nwb_sync(h))
+
+    def evalRhs(self) -> np.ndarray:
+        """M^{-1}(K u + F*) of the current state (the reference's d_rhs_)."""
+        h = self._need()
+        out = np.empty(6 * self._npts)
+        check(_lib.lib().nwb_eval_rhs(h, dptr(out), out.size))
+        return out
+
+    def energy(self) -> float:
+        """FP64 discrete energy 1/2 sum J w3 (|E|^2+|H|^2) (src/case.cpp:733-766)."""
+        h = self._need()
+        e = C.c_double()
+        check(_lib.lib().nwb_energy(h, C.byref(e)))
+        return e.value
+
+    def info(self) -> dict:
+        h = self._need()
+        i = SolverInfo()
+        check(_lib.lib().nwb_solver_get_info(h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in SolverInfo._fields_}
+
+    def launchCount(self) -> int:
+        n = C.c_longlong()
+        check(_lib.lib().nwb_solver_launch_count(self._need(), C.byref(n)))
+        return n.value
+
+    def timeSteps(self, dt: float, nsteps: int, graph: bool = True) -> float:
+        """Device time (ms) of nsteps steps, CUDA events on the solver's stream."""
+        ms = C.c_float()
+        check(_lib.lib().nwb_time_steps(self._need(), float(dt), int(nsteps), int(graph),
+                                        C.byref(ms)))
+        return ms.value
+
+    def timeStageKernel(self, dt: float, nstages: int) -> float:
+        """Average device time (ms) of one fused stage kernel over nstages launches."""
+        ms = C.c_float()
+        check(_lib.lib().nwb_time_stage_kernel(self._need(), float(dt), int(nstages),
+                                               C.byref(ms)))
+        return ms.value
+
+    def deviceState(self):
+        """(device pointer of the current state [6][stride], cudaStream_t handle)."""
+        p = _lib._D()
+        s = C.c_void_p()
+        check(_lib.lib().nwb_solver_device_state(self._need(), C.byref(p), C.byref(s)))
+        return C.cast(p, C.c_void_p).value, s.value
+
+    def finalize(self) -> None:
+        """Release device buffers and the stream (DgSolver::finalize)."""
+        if self._h is not None:
+            _lib.lib().nwb_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass

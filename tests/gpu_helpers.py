@@ -1,0 +1,42 @@
+"""Shared helpers of the GPU parity tests (imported by test modules only)."""
+import numpy as np
+
+from nekwave_b200 import DgSolver, Mesh
+from oracle import oracle as O
+
+
+def solver_for(m: "O.MeshArrays", c0: float, precision: str = "fp64") -> DgSolver:
+    """libnwb solver on exactly the oracle's mesh arrays."""
+    mesh = Mesh.from_arrays(m.N, m.nelt, z=m.z, w=m.w, D=m.D, w3=m.w3, jac=m.jac, met=m.met,
+                            vmin=m.vmin, vplus=m.vplus, bc=m.bc, nx=m.nx, ny=m.ny, nz=m.nz,
+                            dA=m.dA, x=m.x, y=m.y, zc=m.zc)
+    s = DgSolver(precision)
+    s.initialize(mesh, c0)
+    s._keep_mesh = mesh
+    return s
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def rel_max(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def random_state(m, seed):
+    return np.random.Generator(np.random.PCG64(seed)).standard_normal(6 * m.npts)
+
+
+def smooth_state(m, seed):
+    """Band-limited seeded fields (Gaussian pulses in all six components)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lo = np.array([m.x.min(), m.y.min(), m.zc.min()])
+    hi = np.array([m.x.max(), m.y.max(), m.zc.max()])
+    u = np.zeros(6 * m.npts)
+    for c in range(6):
+        r0 = lo + (hi - lo) * rng.uniform(0.3, 0.7, 3)
+        sig = 0.15 * float(np.min(hi - lo))
+        u[c * m.npts:(c + 1) * m.npts] = np.exp(-((m.x - r0[0]) ** 2 + (m.y - r0[1]) ** 2 +
+                                                  (m.zc - r0[2]) ** 2) / sig ** 2)
+    return u

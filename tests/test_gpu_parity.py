@@ -1,0 +1,204 @@
+"""Parity of the CUDA path (libnwb, through its C ABI) with the oracle on the
+same seeded inputs, plus the reference's own golden vectors.
+
+FP64 tolerance: the CUDA path contracts a*b+c into FMAs and sums each residual
+in a fixed order that differs from the reference's (its lift is an atomicAdd in
+arbitrary order), so results agree to rounding, not bitwise.  The bound used is
+a relative max error of 1e-12 for one right-hand side and a relative L2 error
+of 1e-12 for a few steps, 1e-10 for 200 steps.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.gpu_helpers import random_state, rel_l2, rel_max, smooth_state, solver_for
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+STEP_TOL = 1e-12
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("N", range(2, 11))
+@pytest.mark.parametrize("c0", [0.0, 1.0])
+def test_rhs_pec_box_all_orders(gpu, N, c0):
+    m = O.box_mesh(N, (3, 2, 2), (0.0, -1.0, 0.0), (1.5, 1.0, 0.75))
+    s = solver_for(m, c0)
+    assert s.info()["geometry"] == 0
+    u = random_state(m, N)
+    s.uploadState(u)
+    got = s.evalRhs()
+    want = O.rhs(m, c0, u)
+    assert rel_max(got, want) < RHS_TOL
+    np.testing.assert_array_equal(s.downloadState(), u)  # evalRhs leaves the state alone
+    s.finalize()
+
+
+@pytest.mark.parametrize("N,nel,per", [(4, (2, 2, 2), (1, 1, 1)), (5, (3, 1, 2), (1, 0, 1)),
+                                       (8, (2, 3, 2), (0, 1, 0)), (7, (1, 1, 1), (1, 1, 1)),
+                                       (3, (5, 4, 3), (0, 0, 1))])
+@pytest.mark.parametrize("c0", [0.0, 0.5, 1.0])
+def test_rhs_periodic_and_mixed(gpu, N, nel, per, c0):
+    m = O.box_mesh(N, nel, (0, 0, 0), (1, 2, 1), per)
+    s = solver_for(m, c0)
+    u = random_state(m, 7)
+    s.uploadState(u)
+    assert rel_max(s.evalRhs(), O.rhs(m, c0, u)) < RHS_TOL
+    s.finalize()
+
+
+@pytest.mark.parametrize("N", [3, 5, 8])
+def test_rhs_affine_parallelepiped(gpu, N):
+    A = [[1.0, 0.3, 0.1], [-0.2, 1.1, 0.05], [0.1, 0.2, 0.9]]
+    m = O.warped_box_mesh(N, (3, 2, 2), linear=A)
+    s = solver_for(m, 1.0)
+    assert s.info()["geometry"] == 1
+    u = random_state(m, 3)
+    s.uploadState(u)
+    assert rel_max(s.evalRhs(), O.rhs(m, 1.0, u)) < RHS_TOL
+    s.finalize()
+
+
+@pytest.mark.parametrize("N", [2, 4, 6, 9])
+@pytest.mark.parametrize("c0", [0.0, 1.0])
+def test_rhs_trilinear_per_node_geometry(gpu, N, c0):
+    m = O.warped_box_mesh(N, (3, 3, 2), warp=0.06)
+    s = solver_for(m, c0)
+    assert s.info()["geometry"] == 2
+    u = random_state(m, 5)
+    s.uploadState(u)
+    assert rel_max(s.evalRhs(), O.rhs(m, c0, u)) < RHS_TOL
+    s.finalize()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_against_reference_golden_vectors(gpu, path):
+    g = np.load(path)
+    m = O.box_mesh(int(g["N"]), tuple(g["nel"]), tuple(g["lo"]), tuple(g["hi"]),
+                   tuple(bool(p) for p in g["periodic"]))
+    c0 = float(g["c0"])
+    s = solver_for(m, c0)
+    s.uploadState(g["u0"])
+    assert rel_max(s.evalRhs(), g["rhs"]) < RHS_TOL
+    for n in range(int(g["steps"])):
+        s.step(float(g["dt"]), 0.0)
+        assert abs(s.energy() - g["energies"][n]) <= 1e-12 * abs(g["energies"][n])
+    assert rel_l2(s.downloadState(), g["u1"]) < STEP_TOL
+    s.finalize()
+
+
+@pytest.mark.parametrize("N,nel,per,c0", [(4, (2, 2, 2), (0, 0, 0), 1.0), (6, (2, 2, 3), (1, 1, 1), 0.0),
+                                          (8, (2, 2, 2), (1, 0, 0), 1.0)])
+@pytest.mark.parametrize("graph", [False, True])
+def test_steps_match_oracle(gpu, N, nel, per, c0, graph):
+    m = O.box_mesh(N, nel, (0, 0, 0), (1, 1, 1), per)
+    s = solver_for(m, c0)
+    u = smooth_state(m, 11)
+    dt = 0.5 * O.dxmin(m)
+    s.uploadState(u)
+    if graph:
+        s.steps(dt, 6)
+    else:
+        for _ in range(6):
+            s.step(dt, 0.0)
+    want, _ = O.step(m, c0, dt, 6, u)
+    assert rel_l2(s.downloadState(), want) < STEP_TOL
+    s.finalize()
+
+
+def tm110_exact(m, T):
+    n, w = m.npts, np.pi * np.sqrt(2.0)
+    ex = np.zeros(6 * n)
+    ex[2 * n:3 * n] = np.sin(np.pi * m.x) * np.sin(np.pi * m.y) * np.cos(w * T)
+    ex[3 * n:4 * n] = -np.sin(np.pi * m.x) * np.cos(np.pi * m.y) * np.sin(w * T) / np.sqrt(2.0)
+    ex[4 * n:5 * n] = np.cos(np.pi * m.x) * np.sin(np.pi * m.y) * np.sin(w * T) / np.sqrt(2.0)
+    return ex
+
+
+def test_tm110_cavity_200_steps(gpu):
+    """PEC unit cube, 4^3 elements, 5 GLL points, upwind, CFL 0.5, 200 LSRK45 steps,
+    Ez = sin(pi x) sin(pi y): the oracle after 200 steps and the analytic TM110 mode."""
+    m = O.box_mesh(5, (4, 4, 4), (0, 0, 0), (1, 1, 1))
+    dt = 0.5 * O.dxmin(m)
+    u0 = tm110_exact(m, 0.0)
+    s = solver_for(m, 1.0)
+    s.uploadState(u0)
+    s.steps(dt, 200)
+    got = s.downloadState()
+    want, _ = O.step(m, 1.0, dt, 200, u0)
+    assert rel_l2(got, want) < 1e-10
+    assert rel_l2(got, tm110_exact(m, 200 * dt)) < 5e-5
+    e0 = O.energy(m, u0)
+    assert s.energy() <= e0  # upwind never gains energy
+    s.finalize()
+
+
+def test_upwind_energy_monotone_stability_case(gpu):
+    """MaxwellStabilityTest (tests/nekwave_test.cpp:212-293): N=4, 2x2x2 on
+    [-0.5,0.5]^3, upwind, Ez = exp(-50 r^2), dt = 0.005, energy never increases."""
+    m = O.box_mesh(4, (2, 2, 2), (-.5, -.5, -.5), (.5, .5, .5))
+    u = np.zeros(6 * m.npts)
+    u[2 * m.npts:3 * m.npts] = np.exp(-50.0 * (m.x ** 2 + m.y ** 2 + m.zc ** 2))
+    s = solver_for(m, 1.0)
+    s.uploadState(u)
+    prev = s.energy()
+    assert abs(prev - O.energy(m, u)) <= 1e-13 * prev
+    for _ in range(20):
+        s.step(0.005, 0.0)
+        e = s.energy()
+        assert np.isfinite(e) and e <= prev + 1e-12
+        prev = e
+    s.finalize()
+
+
+def test_central_flux_conserves_energy_periodic(gpu):
+    m = O.box_mesh(6, (4, 4, 4), (0, 0, 0), (1, 1, 1), (True, True, True))
+    u = smooth_state(m, 2)
+    s = solver_for(m, 0.0)
+    s.uploadState(u)
+    e0 = s.energy()
+    s.steps(0.5 * O.dxmin(m), 100)
+    e1 = s.energy()
+    # only the O(dt^5) dissipation of LSRK45 remains
+    assert abs(e1 - e0) / e0 < 1e-6
+    s.finalize()
+
+
+def test_bitwise_deterministic(gpu):
+    m = O.box_mesh(6, (4, 3, 3), (0, 0, 0), (1, 1, 1), (True, False, False))
+    u = random_state(m, 1)
+    outs = []
+    for _ in range(2):
+        s = solver_for(m, 1.0)
+        s.uploadState(u)
+        s.steps(1e-3, 5)
+        outs.append(s.downloadState())
+        s.finalize()
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
+def test_rhs_linearity_full_size_c3(gpu):
+    """Size-independent property at the PEC cavity size (64x64x32, 6 points):
+    RHS(a u + b v) = a RHS(u) + b RHS(v) to rounding."""
+    from nekwave_b200 import DgSolver, Mesh
+    mesh = Mesh(6)
+    mesh.createBoxMesh(64, 64, 32, 0.0, 2.0, 0.0, 2.0, 0.0, 1.0)
+    s = DgSolver()
+    s.initialize(mesh, 1.0)
+    rng = np.random.Generator(np.random.PCG64(0))
+    n = 6 * mesh.getTotalPoints()
+    u = rng.standard_normal(n)
+    v = rng.standard_normal(n)
+    s.uploadState(u)
+    ru = s.evalRhs()
+    s.uploadState(v)
+    rv = s.evalRhs()
+    s.uploadState(2.0 * u - 0.5 * v)
+    rw = s.evalRhs()
+    assert rel_l2(rw, 2.0 * ru - 0.5 * rv) < 1e-13
+    s.finalize()
