@@ -47,6 +47,12 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--nel", type=int, default=32,
+                   help="elements per axis; values other than 32 are for profiling only")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="stage-kernel launch shape; -1 = autotune on the workload")
+    p.add_argument("--profile", action="store_true",
+                   help="only warm-up + timed steps (small case for ncu captures)")
     return p.parse_args()
 
 
@@ -242,19 +248,32 @@ def main():
         torch.cuda.synchronize()
 
     N = WORKLOAD["N"]
+    nel = (args.nel,) * 3
     mesh = Mesh(N)
-    mesh.createBoxMesh(*WORKLOAD["nel"], 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, True, True, True)
+    mesh.createBoxMesh(*nel, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, True, True, True)
     npts = mesh.getTotalPoints()
     dt = WORKLOAD["cfl"] * mesh.computeMinNodeDistance()
     u0 = initial_state(mesh.getCoordX(), mesh.getCoordY(), mesh.getCoordZ(), args.seed + rank)
     solver = DgSolver(args.precision)
     solver.initialize(mesh, WORKLOAD["c0"])
     solver.uploadState(u0)
+    tune_ms = None
+    if args.variant >= 0:
+        solver.setVariant(args.variant)
+    else:
+        _, tune_ms = solver.autotune(reps=10)
     info = solver.info()
 
     # warm-up (graphs captured here)
     solver.steps(dt, args.warmup)
     barrier()
+    if args.profile:
+        solver.steps(dt, args.steps)
+        barrier()
+        print(json.dumps({"profile": True, "nel": nel, "npts": npts, "steps": args.steps,
+                          "energy": solver.energy()}))
+        solver.finalize()
+        return
 
     # ---- timed region: K steps, inputs resident in HBM (3 x 805 MB > L2) ---------------
     launches0 = solver.launchCount()
@@ -316,14 +335,17 @@ def main():
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
             "data": "synthetic (seeded Gaussian pulse)",
-            "config": dict(workload=WORKLOAD["workload"], N=N, order=N - 1,
-                           nel=list(WORKLOAD["nel"]), npts=npts, dof=6 * npts,
+            "config": dict(workload=WORKLOAD["workload"] if args.nel == 32 else
+                           f"periodic_box_{args.nel}^3_N8_central", N=N, order=N - 1,
+                           nel=list(nel), npts=npts, dof=6 * npts,
                            flux="central", cfl=WORKLOAD["cfl"], dt=dt,
                            precision=args.precision, parallelism=f"replicas x{world}",
                            l2="inputs larger than L2 (u_in, u_out, k: 3 x 805 MB)",
-                           kernel=dict(ks=info["ks"], epb=info["epb"],
+                           kernel=dict(variant=info["variant"], ks=info["ks"], epb=info["epb"],
+                                       k_in_smem=info["ksmem"], minb=info["minb"],
                                        threads=info["threads_per_block"],
-                                       smem=info["smem_bytes"], geometry=info["geometry"])),
+                                       smem=info["smem_bytes"], geometry=info["geometry"],
+                                       autotune_ms=tune_ms)),
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -136,8 +136,19 @@ typedef struct nwb_solver_info {
     int threads_per_block;
     int smem_bytes;
     long long device_bytes;       /* device memory the solver holds                */
+    int ksmem;                    /* 1: LSRK register staged in shared memory      */
+    int minb;                     /* resident blocks the launch shape asks for     */
+    int variant;                  /* current launch shape                          */
+    int variant_count;            /* launch shapes available for this mesh         */
 } nwb_solver_info;
 nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info);
+/* Launch shape of the fused stage kernel.  nwb_solver_autotune times every
+ * shape for this mesh (reps launches each, with a = b = dt = 0 so the state is
+ * left as it was) and keeps the fastest; ms_out (optional, ms_cap entries)
+ * receives the per-shape average launch time.  Neither call has a counterpart
+ * in the reference, which has one fixed launch shape per kernel. */
+nwb_status nwb_solver_set_variant(nwb_solver* s, int variant);
+nwb_status nwb_solver_autotune(nwb_solver* s, int reps, int* best, float* ms_out, int ms_cap);
 /* Device pointer of the current state ([6][stride] doubles) and the solver's
  * CUDA stream (a cudaStream_t), for callers that keep data on the device. */
 nwb_status nwb_solver_device_state(nwb_solver* s, double** d_state, void** stream);

@@ -48,7 +48,8 @@ class SolverInfo(C.Structure):
     _fields_ = [("N", C.c_int), ("nelt", C.c_int), ("npts", C.c_longlong),
                 ("stride", C.c_longlong), ("geometry", C.c_int), ("precision", C.c_int),
                 ("ks", C.c_int), ("epb", C.c_int), ("threads_per_block", C.c_int),
-                ("smem_bytes", C.c_int), ("device_bytes", C.c_longlong)]
+                ("smem_bytes", C.c_int), ("device_bytes", C.c_longlong), ("ksmem", C.c_int),
+                ("minb", C.c_int), ("variant", C.c_int), ("variant_count", C.c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/nwb.h declares.
@@ -75,6 +76,9 @@ SIGNATURES = {
     "nwb_solver_get_info": (C.c_int, [C.c_void_p, C.POINTER(SolverInfo)]),
     "nwb_solver_device_state": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(C.c_void_p)]),
     "nwb_solver_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "nwb_solver_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "nwb_solver_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_float), C.c_int]),
     "nwb_time_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int,
                                  C.POINTER(C.c_float)]),
     "nwb_time_stage_kernel": (C.c_int, [C.c_void_p, C.c_double, C.c_int,

@@ -213,6 +213,7 @@ struct nwb_solver {
     void* dflush = nullptr;
     size_t flush_bytes = 0;
     nwb::StageConfig cfg{};
+    int variant = 0;
     long long launches = 0;
     size_t device_bytes = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -242,7 +243,7 @@ struct nwb_solver {
 
     nwb_status launch_stage(int stage, double dt) {
         nwb::StageParams P = params(stage, dt);
-        cudaError_t e = nwb::launch_stage(N, geo, f32, P, st, nullptr);
+        cudaError_t e = nwb::launch_stage(N, geo, f32, variant, &P, st, nullptr);
         if (e != cudaSuccess) return fail(NWB_ECUDA, "stage kernel launch: %s", cudaGetErrorString(e));
         cur ^= 1;
         ++launches;
@@ -399,7 +400,7 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
     ce = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce)));
 
-    ce = nwb::stage_config(N, s->geo, s->f32, &s->cfg);
+    ce = nwb::launch_stage(N, s->geo, s->f32, s->variant, nullptr, nullptr, &s->cfg);
     if (ce != cudaSuccess)
         return bail(fail(NWB_ECUDA, "stage kernel set-up: %s", cudaGetErrorString(ce)));
 
@@ -515,7 +516,7 @@ nwb_status nwb_eval_rhs(nwb_solver* s, double* h, size_t n) {
     nwb::StageParams P = s->params(0, 1.0);
     P.a = 0.0;
     P.b = 0.0;
-    cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, P, s->st, nullptr);
+    cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, s->variant, &P, s->st, nullptr);
     if (e != cudaSuccess) return fail(NWB_ECUDA, "stage kernel launch: %s", cudaGetErrorString(e));
     ++s->launches;
     NWB_CU(cudaMemcpy2DAsync(h, sizeof(double) * s->npts, s->k, sizeof(double) * s->stride,
@@ -557,6 +558,10 @@ nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info) {
     info->epb = s->cfg.epb;
     info->threads_per_block = s->cfg.threads;
     info->smem_bytes = s->cfg.smem;
+    info->ksmem = s->cfg.ksmem;
+    info->minb = s->cfg.minb;
+    info->variant = s->variant;
+    info->variant_count = nwb::stage_variant_count(s->N, s->geo);
     info->device_bytes = static_cast<long long>(s->device_bytes);
     return NWB_OK;
 }
@@ -572,6 +577,67 @@ nwb_status nwb_solver_launch_count(const nwb_solver* s, long long* count) {
     if (!s || !count) return fail(NWB_EINVAL, "nwb_solver_launch_count: null argument");
     *count = s->launches;
     return NWB_OK;
+}
+
+nwb_status nwb_solver_set_variant(nwb_solver* s, int variant) {
+    if (!s) return fail(NWB_EINVAL, "nwb_solver_set_variant: null solver");
+    if (variant < 0 || variant >= nwb::stage_variant_count(s->N, s->geo))
+        return fail(NWB_EINVAL, "nwb_solver_set_variant: variant %d out of range", variant);
+    nwb::StageConfig c{};
+    cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, variant, nullptr, nullptr, &c);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "variant set-up: %s", cudaGetErrorString(e));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    s->variant = variant;
+    s->cfg = c;
+    s->drop_graphs();
+    return NWB_OK;
+}
+
+// Times every launch shape of the stage kernel on this solver's mesh and keeps
+// the fastest.  The timed launches use a = b = dt = 0, so they leave the state
+// bit for bit as it was and reset the LSRK register to zero (which the first
+// stage of every step multiplies by a = 0 anyway).
+nwb_status nwb_solver_autotune(nwb_solver* s, int reps, int* best, float* ms_out, int ms_cap) {
+    if (!s || reps < 1) return fail(NWB_EINVAL, "nwb_solver_autotune: bad argument");
+    const int nv = nwb::stage_variant_count(s->N, s->geo);
+    cudaEvent_t a, b;
+    NWB_CU(cudaEventCreate(&a));
+    NWB_CU(cudaEventCreate(&b));
+    int bestv = s->variant;
+    float bestt = 1e30f;
+    for (int v = 0; v < nv; ++v) {
+        nwb::StageConfig c{};
+        cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, v, nullptr, nullptr, &c);
+        if (e != cudaSuccess) return fail(NWB_ECUDA, "variant set-up: %s", cudaGetErrorString(e));
+        nwb::StageParams P = s->params(0, 0.0);
+        P.a = 0.0;
+        P.b = 0.0;
+        P.u_out = s->u[s->cur ^ 1];
+        for (int w = 0; w < 2; ++w) {
+            e = nwb::launch_stage(s->N, s->geo, s->f32, v, &P, s->st, nullptr);
+            if (e != cudaSuccess) return fail(NWB_ECUDA, "autotune launch: %s", cudaGetErrorString(e));
+        }
+        NWB_CU(cudaEventRecord(a, s->st));
+        for (int r = 0; r < reps; ++r) {
+            e = nwb::launch_stage(s->N, s->geo, s->f32, v, &P, s->st, nullptr);
+            if (e != cudaSuccess) return fail(NWB_ECUDA, "autotune launch: %s", cudaGetErrorString(e));
+        }
+        NWB_CU(cudaEventRecord(b, s->st));
+        NWB_CU(cudaEventSynchronize(b));
+        float t = 0.f;
+        NWB_CU(cudaEventElapsedTime(&t, a, b));
+        t /= reps;
+        s->launches += reps + 2;
+        if (ms_out && v < ms_cap) ms_out[v] = t;
+        if (t < bestt) {
+            bestt = t;
+            bestv = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (best) *best = bestv;
+    return nwb_solver_set_variant(s, bestv);
 }
 
 nwb_status nwb_time_steps(nwb_solver* s, double dt, int nsteps, int use_graph, float* ms) {

@@ -53,19 +53,29 @@ struct StageParams {
     double a, b, dt;        // LSRK45 stage coefficients and step
 };
 
-// Launch configuration of the fused stage kernel for one N.
+// Launch configuration of one fused-stage-kernel variant.
 struct StageConfig {
     int ks;       // threads per (i,j) node column
     int epb;      // elements per block
     int threads;  // threads per block
     int smem;     // dynamic shared memory bytes
+    int ksmem;    // 1: k staged in shared memory, 0: prefetched to L2 and read directly
+    int minb;     // minimum resident blocks requested from the register allocator
 };
 
-// Fused stage kernel launcher (stage_kernels.cu).  Returns cudaErrorInvalidValue
-// when N/geo/precision has no instantiation.
-cudaError_t launch_stage(int N, int geo, int f32, const StageParams& p, cudaStream_t st,
-                         StageConfig* cfg_out);
-cudaError_t stage_config(int N, int geo, int f32, StageConfig* cfg);
+// Fused stage kernel (stage_inst.cu, one object per N).  Variant 0 exists for
+// every (N, geometry, precision); the axis-aligned class has more variants,
+// which the autotuner times.  Returns cudaErrorInvalidValue for an unknown
+// combination.  p == nullptr only reports the configuration (and performs the
+// one-time kernel attribute set-up).
+cudaError_t launch_stage(int N, int geo, int f32, int variant, const StageParams* p,
+                         cudaStream_t st, StageConfig* cfg_out);
+int stage_variant_count(int N, int geo);
+template <int N>
+cudaError_t launch_stage_n(int geo, int f32, int variant, const StageParams* p, cudaStream_t st,
+                           StageConfig* cfg);
+template <int N>
+int stage_variant_count_n(int geo);
 
 // FP64 energy of the state u (diag_kernels.cu): nblocks partial sums, then one
 // fixed-order final sum into *out (device).  J comes from jac_e (per element,

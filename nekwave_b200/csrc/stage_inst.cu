@@ -1,0 +1,83 @@
+// stage_inst.cu -- instantiations of the fused stage kernel for one N.
+// Compiled once per N (2..10) with -DNWB_N=<N> so the objects build in parallel.
+#include "stage_kernel.cuh"
+#include "stage_variants.h"
+
+#ifndef NWB_N
+#error "compile with -DNWB_N=<points per direction>"
+#endif
+
+#define NWB_CAT2(a, b) a##b
+#define NWB_CAT(a, b) NWB_CAT2(a, b)
+#define NWB_VLIST NWB_CAT(NWB_VARIANTS_, NWB_N)
+
+namespace nwb {
+namespace stage {
+// Everything below depends on NWB_N and differs between the per-N objects, so
+// it must have internal linkage (one-definition rule across the objects).
+namespace {
+
+struct Shape {
+    int ks, epb, ksm, minb;
+};
+#define NWB_X(ks, epb, ksm, minb) Shape{ks, epb, ksm, minb},
+constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
+#undef NWB_X
+constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
+
+// every variant for the axis-aligned class, variant 0 for the others
+template <int GEO, bool F32, int I>
+cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, StageConfig* cfg) {
+    if constexpr (I < kNumShapes) {
+        if (vid == I) {
+            if constexpr (GEO == GEO_BOX || I == 0) {
+                constexpr Shape v = kShapes[I];
+                return launch_cfg<NWB_N, GEO, F32, v.ks, v.epb, (v.ksm != 0), v.minb>(p, st, cfg);
+            } else {
+                return cudaErrorInvalidValue;
+            }
+        }
+        return launch_variant<GEO, F32, I + 1>(vid, p, st, cfg);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <int GEO>
+int count_variants() {
+    return GEO == GEO_BOX ? kNumShapes : 1;
+}
+
+}  // namespace
+}  // namespace stage
+
+template <>
+cudaError_t launch_stage_n<NWB_N>(int geo, int f32, int variant, const StageParams* p,
+                                  cudaStream_t st, StageConfig* cfg) {
+    using namespace stage;
+    switch (geo) {
+        case GEO_BOX:
+            return f32 ? launch_variant<GEO_BOX, true, 0>(variant, p, st, cfg)
+                       : launch_variant<GEO_BOX, false, 0>(variant, p, st, cfg);
+        case GEO_AFFINE:
+            return f32 ? launch_variant<GEO_AFFINE, true, 0>(variant, p, st, cfg)
+                       : launch_variant<GEO_AFFINE, false, 0>(variant, p, st, cfg);
+        case GEO_NODAL:
+            return f32 ? launch_variant<GEO_NODAL, true, 0>(variant, p, st, cfg)
+                       : launch_variant<GEO_NODAL, false, 0>(variant, p, st, cfg);
+        default:
+            return cudaErrorInvalidValue;
+    }
+}
+
+template <>
+int stage_variant_count_n<NWB_N>(int geo) {
+    switch (geo) {
+        case GEO_BOX: return stage::count_variants<GEO_BOX>();
+        case GEO_AFFINE: return stage::count_variants<GEO_AFFINE>();
+        case GEO_NODAL: return stage::count_variants<GEO_NODAL>();
+        default: return 0;
+    }
+}
+
+}  // namespace nwb

@@ -1,4 +1,4 @@
-// stage_kernels.cu -- the fused LSRK45 stage kernel for sm_100a.
+// stage_kernel.cuh -- the fused LSRK45 stage kernel for sm_100a.
 //
 // One launch performs, for every element, everything the reference does in
 // seven launches per stage (src/dg_solver.cpp:393-505):
@@ -12,8 +12,9 @@
 // Block = EPB elements; each element is handled by a team of KS*N*N threads,
 // thread (i,j,h) owning node column (i,j) for the planes k of its share h.
 // Per block:
-//   1. cp.async stages u_in and k of the EPB elements in shared memory
-//      (two commit groups, so k arrives while the flux and volume work runs);
+//   1. cp.async stages u_in of the EPB elements in shared memory; k is either
+//      staged too (second commit group, it arrives while the flux and volume
+//      work runs) or prefetched into L2 and read directly by its owner thread;
 //   2. face phase: one thread per face point computes the numerical flux from
 //      its own trace (shared memory) and the neighbour trace (shared memory if
 //      the neighbour is in the same block, else global/L2), multiplies it by the
@@ -23,12 +24,13 @@
 //      LSRK update in FP64, and coalesced stores of k and u_out.
 // Each residual entry is formed once by one thread in a fixed order: the
 // kernel is deterministic (the reference's atomic lift is not).
+#pragma once
 #include "nwb_internal.h"
 
 #include <type_traits>
 
 namespace nwb {
-namespace {
+namespace stage {
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -58,12 +60,12 @@ __device__ __forceinline__ int face_local(int f, int p, int q) {
 
 constexpr int align16(int b) { return (b + 15) & ~15; }
 
-template <int N, bool F32, int EPB>
+template <int N, bool F32, int EPB, bool KSMEM>
 struct SmemLayout {
     static constexpr int N2 = N * N, N3 = N2 * N;
     static constexpr int u = 0;
     static constexpr int k = u + EPB * 6 * N3 * 8;
-    static constexpr int D = k + EPB * 6 * N3 * 8;
+    static constexpr int D = k + (KSMEM ? EPB * 6 * N3 * 8 : 0);
     static constexpr int geo = D + align16(N2 * 8);
     static constexpr int conn = geo + EPB * static_cast<int>(sizeof(ElemGeo));
     static constexpr int flux = conn + align16(EPB * 6 * 4);
@@ -99,8 +101,8 @@ __device__ __forceinline__ void numerical_flux(T nx, T ny, T nz, T hc0, T dEx, T
     f[5] = -half * nxE_z - hc0 * nnH_z;
 }
 
-template <int N, int GEO, bool F32, int KS, int EPB>
-__global__ void __launch_bounds__(EPB * KS * N * N)
+template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM, int MINB>
+__global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage_kernel(const StageParams P) {
     using TC = typename std::conditional<F32, float, double>::type;
     constexpr int N2 = N * N, N3 = N2 * N;
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N)
     constexpr int NT = EPB * TPE;         // threads per block
     constexpr int KPT = (N + KS - 1) / KS;
     constexpr int CS = EPB * N3;          // component stride in shared memory
-    using L = SmemLayout<N, F32, EPB>;
+    using L = SmemLayout<N, F32, EPB, KSMEM>;
 
     extern __shared__ __align__(16) unsigned char smem[];
     double* s_u = reinterpret_cast<double*>(smem + L::u);
@@ -152,10 +154,21 @@ __global__ void __launch_bounds__(EPB * KS * N * N)
             for (int x = tid; x < nvalid * 6; x += NT) s_conn[x] = P.conn[e0 * 6 + x];
         }
         cp_async_commit();
+        if constexpr (KSMEM) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const double* src = P.k + c * S + gbase;
-            for (int x = tid; x < cnt; x += NT) cp_async8(s_k + c * CS + x, src + x);
+            for (int c = 0; c < 6; ++c) {
+                const double* src = P.k + c * S + gbase;
+                for (int x = tid; x < cnt; x += NT) cp_async8(s_k + c * CS + x, src + x);
+            }
+        } else {
+            // pull this block's k lines into L2 now; the owner threads read them
+            // in the column phase
+            const int lines = (cnt * 8 + 127) / 128;
+            for (int x = tid; x < 6 * lines; x += NT) {
+                const int c = x / lines, ln = x - c * lines;
+                const double* a = P.k + c * S + gbase + ln * 16;
+                asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a));
+            }
         }
         cp_async_commit();
     }
@@ -363,36 +376,26 @@ __global__ void __launch_bounds__(EPB * KS * N * N)
         // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
         const int sl = team * N3 + mloc;
         const long long g = ebase + mloc;
+        double kold[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) kold[c] = KSMEM ? s_k[c * CS + sl] : __ldcg(P.k + c * S + g);
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            const double kn = A * s_k[c * CS + sl] + DT * rhs[c];
-            P.k[c * S + g] = kn;
-            P.u_out[c * S + g] = s_u[c * CS + sl] + B * kn;
+            const double kn = A * kold[c] + DT * rhs[c];
+            __stcs(P.k + c * S + g, kn);
+            __stcs(P.u_out + c * S + g, s_u[c * CS + sl] + B * kn);
         }
     }
 }
 
-// Per-N launch shape: threads per column (KS) and elements per block (EPB).
-template <int N> struct Shape;
-template <> struct Shape<2> { static constexpr int KS = 2, EPB = 16; };
-template <> struct Shape<3> { static constexpr int KS = 3, EPB = 8; };
-template <> struct Shape<4> { static constexpr int KS = 2, EPB = 4; };
-template <> struct Shape<5> { static constexpr int KS = 1, EPB = 4; };
-template <> struct Shape<6> { static constexpr int KS = 2, EPB = 2; };
-template <> struct Shape<7> { static constexpr int KS = 1, EPB = 2; };
-template <> struct Shape<8> { static constexpr int KS = 2, EPB = 1; };
-template <> struct Shape<9> { static constexpr int KS = 1, EPB = 1; };
-template <> struct Shape<10> { static constexpr int KS = 1, EPB = 1; };
-
-template <int N, int GEO, bool F32>
-cudaError_t launch_n(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
-    constexpr int KS = Shape<N>::KS, EPB = Shape<N>::EPB;
+// Launch of one variant.  The opt-in shared-memory size is set on the first
+// call, which the solver makes at creation (outside any stream capture).
+template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM, int MINB>
+cudaError_t launch_cfg(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int threads = EPB * KS * N * N;
-    constexpr int smem = SmemLayout<N, F32, EPB>::total;
-    auto kern = stage_kernel<N, GEO, F32, KS, EPB>;
-    if (cfg) *cfg = StageConfig{KS, EPB, threads, smem};
-    // The opt-in shared-memory size is set on the first call, which the solver
-    // makes at creation (outside any stream capture).
+    constexpr int smem = SmemLayout<N, F32, EPB, KSMEM>::total;
+    auto kern = stage_kernel<N, GEO, F32, KS, EPB, KSMEM, MINB>;
+    if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, KSMEM ? 1 : 0, MINB};
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -405,44 +408,5 @@ cudaError_t launch_n(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     return cudaGetLastError();
 }
 
-template <int N>
-cudaError_t dispatch_geo(int geo, int f32, const StageParams* p, cudaStream_t st, StageConfig* c) {
-    switch (geo) {
-        case GEO_BOX:
-            return f32 ? launch_n<N, GEO_BOX, true>(p, st, c) : launch_n<N, GEO_BOX, false>(p, st, c);
-        case GEO_AFFINE:
-            return f32 ? launch_n<N, GEO_AFFINE, true>(p, st, c) : launch_n<N, GEO_AFFINE, false>(p, st, c);
-        case GEO_NODAL:
-            return f32 ? launch_n<N, GEO_NODAL, true>(p, st, c) : launch_n<N, GEO_NODAL, false>(p, st, c);
-        default:
-            return cudaErrorInvalidValue;
-    }
-}
-
-cudaError_t dispatch(int N, int geo, int f32, const StageParams* p, cudaStream_t st, StageConfig* c) {
-    switch (N) {
-        case 2: return dispatch_geo<2>(geo, f32, p, st, c);
-        case 3: return dispatch_geo<3>(geo, f32, p, st, c);
-        case 4: return dispatch_geo<4>(geo, f32, p, st, c);
-        case 5: return dispatch_geo<5>(geo, f32, p, st, c);
-        case 6: return dispatch_geo<6>(geo, f32, p, st, c);
-        case 7: return dispatch_geo<7>(geo, f32, p, st, c);
-        case 8: return dispatch_geo<8>(geo, f32, p, st, c);
-        case 9: return dispatch_geo<9>(geo, f32, p, st, c);
-        case 10: return dispatch_geo<10>(geo, f32, p, st, c);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-}  // namespace
-
-cudaError_t launch_stage(int N, int geo, int f32, const StageParams& p, cudaStream_t st,
-                         StageConfig* cfg_out) {
-    return dispatch(N, geo, f32, &p, st, cfg_out);
-}
-
-cudaError_t stage_config(int N, int geo, int f32, StageConfig* cfg) {
-    return dispatch(N, geo, f32, nullptr, nullptr, cfg);
-}
-
+}  // namespace stage
 }  // namespace nwb

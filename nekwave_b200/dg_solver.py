@@ -111,6 +111,18 @@ class DgSolver:
         check(_lib.lib().nwb_solver_launch_count(self._need(), C.byref(n)))
         return n.value
 
+    def setVariant(self, variant: int) -> None:
+        check(_lib.lib().nwb_solver_set_variant(self._need(), int(variant)))
+
+    def autotune(self, reps: int = 10):
+        """Time every launch shape on this mesh, keep the fastest; returns
+        (best variant, per-variant ms)."""
+        n = self.info()["variant_count"]
+        ms = (C.c_float * n)()
+        best = C.c_int()
+        check(_lib.lib().nwb_solver_autotune(self._need(), int(reps), C.byref(best), ms, n))
+        return best.value, [float(x) for x in ms]
+
     def timeSteps(self, dt: float, nsteps: int, graph: bool = True) -> float:
         """Device time (ms) of nsteps steps, CUDA events on the solver's stream."""
         ms = C.c_float()

@@ -157,15 +157,28 @@ def test_upwind_energy_monotone_stability_case(gpu):
 
 
 def test_central_flux_conserves_energy_periodic(gpu):
+    """Central flux on a periodic box: the semi-discrete operator conserves the
+    discrete energy (u^T M rhs(u) = 0 to rounding), the fully discrete drift is the
+    LSRK45 dissipation (it shrinks ~32x when dt halves) and matches the oracle."""
     m = O.box_mesh(6, (4, 4, 4), (0, 0, 0), (1, 1, 1), (True, True, True))
     u = smooth_state(m, 2)
     s = solver_for(m, 0.0)
     s.uploadState(u)
+    r = s.evalRhs()
+    wts = np.tile(m.jac * np.tile(m.w3, m.nelt), 6)
+    assert abs(np.sum(u * wts * r)) / np.sum(u * wts * u) < 1e-14
     e0 = s.energy()
-    s.steps(0.5 * O.dxmin(m), 100)
-    e1 = s.energy()
-    # only the O(dt^5) dissipation of LSRK45 remains
-    assert abs(e1 - e0) / e0 < 1e-6
+    dt = 0.5 * O.dxmin(m)
+    drifts = []
+    for f in (1, 2):
+        s.uploadState(u)
+        s.steps(dt / f, 100 * f)
+        e1 = s.energy()
+        want, _ = O.step(m, 0.0, dt / f, 100 * f, u)
+        assert abs(e1 - O.energy(m, want)) <= 1e-12 * e0
+        drifts.append((e0 - e1) / e0)
+    assert drifts[0] > 0 and drifts[1] > 0
+    assert 20.0 < drifts[0] / drifts[1] < 45.0
     s.finalize()
 
 
@@ -201,4 +214,31 @@ def test_rhs_linearity_full_size_c3(gpu):
     s.uploadState(2.0 * u - 0.5 * v)
     rw = s.evalRhs()
     assert rel_l2(rw, 2.0 * ru - 0.5 * rv) < 1e-13
+    s.finalize()
+
+
+@pytest.mark.parametrize("N", range(2, 11))
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_every_launch_shape_matches_oracle(gpu, N, prec):
+    """Each launch shape the autotuner may pick computes the same stage."""
+    m = O.box_mesh(N, (3, 3, 2), (0, 0, 0), (1, 1, 1), (True, False, True))
+    s = solver_for(m, 1.0, prec)
+    u = random_state(m, 9)
+    s.uploadState(u)
+    want = O.rhs(m, 1.0, u)
+    dt = 0.5 * O.dxmin(m)
+    want_steps, _ = O.step(m, 1.0, dt, 2, u)
+    tol = RHS_TOL if prec == "fp64" else 1e-4
+    nv = s.info()["variant_count"]
+    assert nv >= 3
+    for v in range(nv):
+        s.setVariant(v)
+        s.uploadState(u)
+        assert rel_max(s.evalRhs(), want) < tol, v
+        s.steps(dt, 2)
+        assert rel_l2(s.downloadState(), want_steps) < (STEP_TOL if prec == "fp64" else 1e-5), v
+    s.uploadState(u)
+    best, ms = s.autotune(reps=3)
+    assert 0 <= best < nv and len(ms) == nv and all(t > 0 for t in ms)
+    np.testing.assert_array_equal(s.downloadState(), u)  # autotuning leaves the state alone
     s.finalize()

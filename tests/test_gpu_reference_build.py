@@ -1,0 +1,96 @@
+"""Parity with the reference's own CUDA build (its DgSolver and kernels compiled
+unchanged for sm_100a into oracle/_ref/libnwref_cuda.so) on the same B200, and
+the reference's step time on the same workload.
+
+FP64 tolerance: the reference lifts face fluxes with atomicAdd in arbitrary
+order, so it is not bit-reproducible itself; its run-to-run spread is measured
+here and the new path must agree with it to 1e-12 relative L2 (1e-10 after 200
+steps)."""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.gpu_helpers import rel_l2, smooth_state, solver_for
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_gpu_available(), reason="reference CUDA build absent")]
+
+OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
+
+
+def ref_gpu_run(N, nel, lo, hi, per, c0, u0, dt, nsteps):
+    L = O.ref_gpu()
+    mh = L.nwref_mesh_box(N, nel[0], nel[1], nel[2], lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
+                          int(per[0]), int(per[1]), int(per[2]))
+    s = L.nwref_gpu_create(mh, c0)
+    u = np.ascontiguousarray(u0, dtype=np.float64)
+    L.nwref_gpu_upload(s, O._dp(u), u.size)
+    ms = L.nwref_gpu_steps(s, dt, nsteps)
+    out = np.empty_like(u)
+    L.nwref_gpu_download(s, O._dp(out), out.size)
+    L.nwref_gpu_destroy(s)
+    L.nwref_mesh_free(mh)
+    return out, ms
+
+
+def test_tm110_matches_reference_cuda_build(gpu):
+    N, nel, lo, hi, per = 5, (4, 4, 4), (0, 0, 0), (1, 1, 1), (0, 0, 0)
+    m = O.box_mesh(N, nel, lo, hi, per)
+    dt = 0.5 * O.dxmin(m)
+    n = m.npts
+    u0 = np.zeros(6 * n)
+    u0[2 * n:3 * n] = np.sin(np.pi * m.x) * np.sin(np.pi * m.y)
+    ref_a, _ = ref_gpu_run(N, nel, lo, hi, per, 1.0, u0, dt, 200)
+    ref_b, _ = ref_gpu_run(N, nel, lo, hi, per, 1.0, u0, dt, 200)
+    spread = rel_l2(ref_a, ref_b)
+    s = solver_for(m, 1.0)
+    s.uploadState(u0)
+    s.steps(dt, 200)
+    ours = s.downloadState()
+    s.finalize()
+    err = rel_l2(ours, ref_a)
+    os.makedirs(OUT, exist_ok=True)
+    with open(os.path.join(OUT, "ref_parity_tm110.json"), "w") as f:
+        json.dump({"ref_run_to_run_rel_l2": spread, "ours_vs_ref_rel_l2": err}, f)
+    assert err < 1e-10
+
+
+@pytest.mark.parametrize("N,nel,per,c0", [(8, (4, 4, 4), (1, 1, 1), 0.0), (6, (6, 6, 3), (0, 0, 0), 1.0)])
+def test_random_state_matches_reference_cuda_build(gpu, N, nel, per, c0):
+    lo, hi = (0, 0, 0), (1, 1, 1)
+    m = O.box_mesh(N, nel, lo, hi, per)
+    u0 = smooth_state(m, 4)
+    dt = 0.5 * O.dxmin(m)
+    ref, _ = ref_gpu_run(N, nel, lo, hi, per, c0, u0, dt, 5)
+    s = solver_for(m, c0)
+    s.uploadState(u0)
+    s.steps(dt, 5)
+    assert rel_l2(s.downloadState(), ref) < 1e-12
+    s.finalize()
+
+
+def test_reference_cuda_step_time_on_benchmark_workload(gpu):
+    """Times the reference's own DgSolver::step on the benchmark workload (periodic
+    32^3, 8 points, central) and records it next to ours (gpurun_out/)."""
+    N, nel, per = 8, (32, 32, 32), (1, 1, 1)
+    L = O.ref_gpu()
+    mh = L.nwref_mesh_box(N, *nel, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, *per)
+    s = L.nwref_gpu_create(mh, 0.0)
+    npts = nel[0] * nel[1] * nel[2] * N ** 3
+    u = np.zeros(6 * npts)
+    L.nwref_gpu_upload(s, O._dp(u), u.size)
+    dt = 1e-3
+    L.nwref_gpu_steps(s, dt, 3)
+    ms = L.nwref_gpu_steps(s, dt, 10)
+    L.nwref_gpu_destroy(s)
+    L.nwref_mesh_free(mh)
+    rate = 6 * npts * 5 * 10 / (ms / 1e3) / 1e9
+    os.makedirs(OUT, exist_ok=True)
+    with open(os.path.join(OUT, "ref_gpu_timing.json"), "w") as f:
+        json.dump({"workload": "periodic 32^3 N=8 central", "ms_per_step": ms / 10,
+                   "gdof_stage_per_s": rate}, f)
+    assert rate > 0
