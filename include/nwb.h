@@ -79,6 +79,10 @@ typedef struct nwb_box_mesh nwb_box_mesh;
 const char* nwb_last_error(void);
 const char* nwb_status_string(nwb_status s);
 int nwb_version(void);
+/* Makes device the current CUDA device of libnwb's own runtime for the calling
+ * thread (libnwb links the CUDA runtime statically).  The reference picks the
+ * device in Comm::init (src/comm.cpp:35-47); the DgSolver shim forwards it. */
+nwb_status nwb_set_device(int device);
 
 /* ---- box mesh builder ---------------------------------------------------------
  * Replaces Mesh::createBoxMesh (src/mesh.cpp:683-843) with its geometry

@@ -57,6 +57,7 @@ SIGNATURES = {
     "nwb_last_error": (C.c_char_p, []),
     "nwb_status_string": (C.c_char_p, [C.c_int]),
     "nwb_version": (C.c_int, []),
+    "nwb_set_device": (C.c_int, [C.c_int]),
     "nwb_box_mesh_create": (C.c_int, [C.c_int] * 4 + [C.c_double] * 6 +
                             [C.c_int, C.POINTER(C.c_void_p)]),
     "nwb_box_mesh_desc": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc)]),

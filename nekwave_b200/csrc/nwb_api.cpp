@@ -349,6 +349,11 @@ const char* nwb_status_string(nwb_status s) {
 
 int nwb_version(void) { return NWB_VERSION; }
 
+nwb_status nwb_set_device(int device) {
+    NWB_CU(cudaSetDevice(device));
+    return NWB_OK;
+}
+
 nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision prec, nwb_solver** out) {
     if (!out) return fail(NWB_EINVAL, "nwb_solver_create: out is null");
     *out = nullptr;

@@ -1,0 +1,168 @@
+// dg_solver.cpp -- drop-in implementation of NekWave's DgSolver on libnwb.
+//
+// Implements the reference's own header src/dg_solver.hpp (class DgSolver,
+// src/dg_solver.hpp:35-102) on the C ABI of include/nwb.h, so that the
+// reference's Case, examples and tests link against the B200 path unchanged:
+// build the reference's sources with this file in place of src/dg_solver.cpp and
+// without src/device/, and link libnwb.so (recipe: Makefile next to this file).
+//
+//   DgSolver::initialize    -> nwb_solver_create     (src/dg_solver.cpp:40-241)
+//   DgSolver::uploadState   -> nwb_upload_state      (src/dg_solver.cpp:243-262)
+//   DgSolver::downloadState -> nwb_download_state    (src/dg_solver.cpp:264-283)
+//   DgSolver::step          -> nwb_step + nwb_sync   (src/dg_solver.cpp:306-527)
+//   DgSolver::finalize      -> nwb_solver_destroy    (src/dg_solver.cpp:529-582)
+//
+// The face points are handed over in the canonical (element, face, q, p) order
+// nwb_mesh_desc requires; Mesh::getFaceData lists them per (element, face) in
+// the order of Mesh::m_faces, so they are re-ordered by (elementId, faceId).
+// Like the reference, any failure prints a message and aborts
+// (src/device/gpu_runtime.hpp:146-153).  Environment knobs (no counterpart in
+// the reference): NWB_PRECISION=fp32 selects the FP32-bulk class,
+// NWB_AUTOTUNE=1 times the stage kernel's launch shapes at initialize.
+#include "dg_solver.hpp"
+#include "mesh.hpp"
+#include "nwb.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+void nwb_or_abort(nwb_status s, const char* what) {
+    if (s != NWB_OK) {
+        std::fprintf(stderr, "[NekWave nwb ERROR] %s: %s (%s)\n", what, nwb_status_string(s),
+                     nwb_last_error());
+        std::abort();
+    }
+}
+
+int bc_code(const std::string& t) {
+    // src/dg_solver.cpp:92-98
+    if (t == "PEC" || t == "W" || t == "V" || t == "v") return 1;
+    if (t == "PMC" || t == "SYM" || t == "S" || t == "s") return 2;
+    return 0;
+}
+
+}  // namespace
+
+class DgSolver::Impl {
+public:
+    ~Impl() { freeBuffers(); }
+
+    bool initialize(const Mesh& mesh, double c0) {
+        freeBuffers();
+        if (mesh.isPartitioned() && mesh.getNumHaloPoints() > 0) {
+            std::fprintf(stderr, "[NekWave nwb ERROR] partitioned (MPI) meshes are not supported: "
+                                 "the B200 path is single-GPU\n");
+            std::abort();
+        }
+        const int N = mesh.getN();
+        const int nelt = mesh.getNumElements();
+        const size_t nn = static_cast<size_t>(N) * N;
+        const size_t nfp = 6 * nn * nelt;
+        npts_ = static_cast<size_t>(mesh.getTotalPoints());
+        std::vector<int> vmin(nfp), vplus(nfp), bc(nfp);
+        std::vector<double> nx(nfp), ny(nfp), nz(nfp), dA(nfp);
+        std::vector<char> seen(6 * static_cast<size_t>(nelt), 0);
+        for (const auto& fd : mesh.getFaceData()) {
+            if (fd.elementId < 0 || fd.elementId >= nelt || fd.faceId < 0 || fd.faceId > 5 ||
+                fd.points.size() != nn) {
+                std::fprintf(stderr, "[NekWave nwb ERROR] unexpected face data layout\n");
+                std::abort();
+            }
+            const size_t slot = 6 * static_cast<size_t>(fd.elementId) + fd.faceId;
+            seen[slot] = 1;
+            const int code = bc_code(fd.bcType);
+            for (size_t pq = 0; pq < nn; ++pq) {
+                const FacePointData& pt = fd.points[pq];
+                const size_t fp = slot * nn + pq;
+                vmin[fp] = pt.volIdxMinus;
+                vplus[fp] = pt.volIdxPlus;
+                int c = code;
+                if (pt.volIdxPlus < 0 && c == 0) c = 1;  // src/dg_solver.cpp:101-103
+                bc[fp] = c;
+                nx[fp] = pt.nx;
+                ny[fp] = pt.ny;
+                nz[fp] = pt.nz;
+                dA[fp] = pt.dA;
+            }
+        }
+        for (char s : seen)
+            if (!s) {
+                std::fprintf(stderr, "[NekWave nwb ERROR] mesh has an element face without face data\n");
+                std::abort();
+            }
+        nwb_mesh_desc d{};
+        d.N = N;
+        d.nelt = nelt;
+        d.D = mesh.getD().data();
+        d.w3 = mesh.getW3().data();
+        d.jac = mesh.getJac().data();
+        const std::vector<double>* m[9] = {&mesh.getRx(), &mesh.getSx(), &mesh.getTx(),
+                                           &mesh.getRy(), &mesh.getSy(), &mesh.getTy(),
+                                           &mesh.getRz(), &mesh.getSz(), &mesh.getTz()};
+        for (int c = 0; c < 9; ++c) d.met[c] = m[c]->data();
+        d.vol_idx_minus = vmin.data();
+        d.vol_idx_plus = vplus.data();
+        d.bc_type = bc.data();
+        d.nx = nx.data();
+        d.ny = ny.data();
+        d.nz = nz.data();
+        d.dA = dA.data();
+        // libnwb carries its own CUDA runtime: hand it the device the application
+        // selected (Comm::init binds rank % numGPUs, src/comm.cpp:35-47)
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) nwb_or_abort(nwb_set_device(dev), "DgSolver::initialize");
+        const char* prec = std::getenv("NWB_PRECISION");
+        const nwb_precision p = (prec && std::strcmp(prec, "fp32") == 0) ? NWB_FP32_BULK : NWB_FP64;
+        nwb_or_abort(nwb_solver_create(&d, c0, p, &s_), "DgSolver::initialize");
+        const char* tune = std::getenv("NWB_AUTOTUNE");
+        if (tune && std::strcmp(tune, "1") == 0)
+            nwb_or_abort(nwb_solver_autotune(s_, 5, nullptr, nullptr, 0), "DgSolver::initialize (autotune)");
+        return true;
+    }
+
+    void uploadState(const double* h, size_t size) {
+        nwb_or_abort(nwb_upload_state(need(), h, size), "DgSolver::uploadState");
+    }
+
+    void downloadState(double* h, size_t size) const {
+        nwb_or_abort(nwb_download_state(need(), h, size), "DgSolver::downloadState");
+    }
+
+    void step(double dt, double /*time: unused, as in src/dg_solver.cpp:307*/) {
+        nwb_or_abort(nwb_step(need(), dt, 1), "DgSolver::step");
+        nwb_or_abort(nwb_sync(need()), "DgSolver::step");  // the reference's step blocks
+    }
+
+    void freeBuffers() {
+        if (s_) {
+            nwb_solver_destroy(s_);
+            s_ = nullptr;
+        }
+    }
+
+private:
+    nwb_solver* need() const {
+        if (!s_) {
+            std::fprintf(stderr, "[NekWave nwb ERROR] DgSolver used before initialize\n");
+            std::abort();
+        }
+        return s_;
+    }
+    nwb_solver* s_ = nullptr;
+    size_t npts_ = 0;
+};
+
+DgSolver::DgSolver() : impl_(new Impl()) {}
+DgSolver::~DgSolver() = default;
+bool DgSolver::initialize(const Mesh& mesh, double c0) { return impl_->initialize(mesh, c0); }
+void DgSolver::uploadState(const double* s, size_t n) { impl_->uploadState(s, n); }
+void DgSolver::downloadState(double* s, size_t n) const { impl_->downloadState(s, n); }
+void DgSolver::step(double dt, double t) { impl_->step(dt, t); }
+void DgSolver::finalize() { impl_->freeBuffers(); }

@@ -1,0 +1,47 @@
+"""The reference's own front end on the B200 path: its unit-test binary and its
+CLI, compiled from the reference sources with nekwave_b200/ref_shim/dg_solver.cpp
+in place of src/dg_solver.cpp (nekwave_b200/ref_shim/Makefile -> build/dropin/)."""
+import csv
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "build", "dropin")
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not os.path.exists(os.path.join(DROPIN, "nekwave-test")),
+                                 reason="drop-in binaries not built")]
+
+
+@pytest.mark.parametrize("name", ["MeshQuadratureTest", "ProbeScalingTest", "MaxwellStabilityTest",
+                                  "PeriodicBCTest"])
+def test_reference_unit_tests_on_nwb(gpu, name):
+    r = subprocess.run([os.path.join(DROPIN, "nekwave-test"), name], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "1 passed, 0 failed" in r.stdout
+
+
+def test_reference_cli_case_on_nwb(gpu, tmp_path):
+    """nekwave <case.json>: PEC unit cube, 4^3 elements, 5 points, upwind, CFL 0.5,
+    40 steps through Case::simulate (per-step download, host probes and energy)."""
+    case = {"mesh": {"nelx": 4, "nely": 4, "nelz": 4, "xmin": 0.0, "xmax": 1.0, "ymin": 0.0,
+                     "ymax": 1.0, "zmin": 0.0, "zmax": 1.0},
+            "numerics": {"order": 5, "cfl": 0.5, "flux_type": "upwind"},
+            "time": {"num_steps": 40},
+            "output": {"output_frequency": 5, "output_dir": str(tmp_path / "out"),
+                       "export_fields": False, "export_format": "csv"}}
+    p = tmp_path / "case.json"
+    p.write_text(json.dumps(case))
+    r = subprocess.run([os.path.join(DROPIN, "nekwave"), str(p)], capture_output=True, text=True,
+                       timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    hist = tmp_path / "out" / "energy_history.csv"
+    assert hist.exists(), r.stdout[-2000:]
+    rows = list(csv.reader(open(hist)))
+    energies = [float(x[-1]) for x in rows[1:]]
+    assert len(energies) >= 8
+    assert all(b <= a * (1 + 1e-12) for a, b in zip(energies, energies[1:]))  # upwind decays
