@@ -146,6 +146,27 @@ typedef struct nwb_solver_info {
     int variant_count;            /* launch shapes available for this mesh         */
 } nwb_solver_info;
 nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info);
+/* Energy of a device-resident state without allocating device memory.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc: a
+ * server that admits work against a fixed HBM budget, a host framework whose own
+ * allocator owns all device memory, or a loop where cudaMalloc's implicit device
+ * synchronisation is not acceptable.  Same quantity as nwb_energy, on any state
+ * laid out as [6][stride] doubles (d_state), with J per element (jac_per_node = 0,
+ * d_jac[nelt]) or per node (jac_per_node = 1, d_jac[nelt*N^3]) and w3[N^3], all
+ * device pointers; the energy is written to the device double d_energy, on
+ * stream (a cudaStream_t, 0 = default stream), without waiting.
+ * Scratch: a fixed array of NWB_ENERGY_NOALLOC_MAX_ELEMENTS doubles (1 MiB) in
+ * the library's device memory, present on every GPU that loads the library
+ * until the process exits; meshes with more elements are refused with
+ * NWB_EINVAL.  The first call on a device looks up that array's device address
+ * (once per device, with the device current); make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be ordered by the caller. */
+#define NWB_ENERGY_NOALLOC_MAX_ELEMENTS 131072
+nwb_status nwb_energy_noalloc(const double* d_state, long long stride, int N, int nelt,
+                              const double* d_jac, int jac_per_node, const double* d_w3,
+                              double* d_energy, void* stream);
+
 /* Launch shape of the fused stage kernel.  nwb_solver_autotune times every
  * shape for this mesh (reps launches each, with a = b = dt = 0 so the state is
  * left as it was) and keeps the fastest; ms_out (optional, ms_cap entries)

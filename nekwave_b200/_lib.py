@@ -77,6 +77,8 @@ SIGNATURES = {
     "nwb_solver_get_info": (C.c_int, [C.c_void_p, C.POINTER(SolverInfo)]),
     "nwb_solver_device_state": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(C.c_void_p)]),
     "nwb_solver_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "nwb_energy_noalloc": (C.c_int, [_D, C.c_longlong, C.c_int, C.c_int, _D, C.c_int, _D, _D,
+                                     C.c_void_p]),
     "nwb_solver_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "nwb_solver_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_float), C.c_int]),
