@@ -185,6 +185,55 @@ nwb_status nwb_time_steps(nwb_solver* s, double dt, int nsteps, int use_graph, f
 /* Per-stage-kernel average device time over nstages stage launches (ms). */
 nwb_status nwb_time_stage_kernel(nwb_solver* s, double dt, int nstages, float* ms);
 
+/* ---- cavity pool: many independent cavities resident on one GPU ----------------
+ * No counterpart in the reference, which solves one mesh per process
+ * (Case::simulate, src/case.cpp:529-660).  A pool owns a fixed HBM arena of
+ * hbm_budget_bytes, allocated once at creation; every cavity ("slot") is
+ * sub-allocated from it, so nwb_pool_add never calls cudaMalloc and returns
+ * NWB_EBUSY when the cavity does not fit (admission by HBM budget).
+ * nwb_pool_step advances every uploaded, unfinished slot by up to nsteps steps
+ * with one persistent launch per LSRK stage (whatever each slot's N and element
+ * count), replayed from one CUDA graph per step; a slot stops by itself after
+ * its own nsteps.  Slots take axis-aligned box meshes (nwb_mesh_desc as above),
+ * their own c0 and dt, up to 8 probes given as (element, tensor Lagrange
+ * weights [3][N]) as ProbeManager builds them (src/probe.cpp:33-189), and record
+ * the energy every energy_every steps (index 0 = initial state, NaN where not
+ * recorded) and all six probe components every step.  Each slot's arithmetic is
+ * the single-mesh stage kernel's, independent of the other slots. */
+typedef struct nwb_pool nwb_pool;
+nwb_status nwb_pool_create(size_t hbm_budget_bytes, int max_slots, nwb_precision precision,
+                           nwb_pool** out);
+nwb_status nwb_pool_add(nwb_pool* p, const nwb_mesh_desc* mesh, double c0, double dt, int nsteps,
+                        int nprobes, const int* probe_elem, const double* probe_w,
+                        int energy_every, int* slot);
+/* Box cavity built inside the library: the geometry of Mesh::createBoxMesh
+ * (src/mesh.cpp:683-843) computed per element from the box parameters (no
+ * per-node arrays on the host), probes given as physical points located as
+ * ProbeManager::init does (src/probe.cpp:33-96). */
+nwb_status nwb_pool_add_box(nwb_pool* p, int N, int nelx, int nely, int nelz, double xmin,
+                            double xmax, double ymin, double ymax, double zmin, double zmax,
+                            int periodic_mask, double c0, double dt, int nsteps, int nprobes,
+                            const double* probe_xyz, int energy_every, int* slot);
+/* Initial state of a box cavity generated on the device: component c is
+ * pulse[5c] * exp(-|x - (pulse[5c+1], pulse[5c+2], pulse[5c+3])|^2 / pulse[5c+4]^2)
+ * (0 where pulse[5c+4] <= 0).  Like nwb_pool_upload, it starts the slot. */
+nwb_status nwb_pool_init_pulse(nwb_pool* p, int slot, const double* pulse /* [30] */);
+/* Initial state [6*npts]; the slot starts stepping with the next nwb_pool_step. */
+nwb_status nwb_pool_upload(nwb_pool* p, int slot, const double* host_state, size_t n);
+nwb_status nwb_pool_step(nwb_pool* p, int nsteps);      /* asynchronous */
+nwb_status nwb_pool_sync(nwb_pool* p);
+/* status[s]: -1 free, 0 added (no state yet), 1 running, 2 finished; done[s]:
+ * steps taken.  Synchronises the pool's stream. */
+nwb_status nwb_pool_query(nwb_pool* p, int* status, int* done, int cap);
+/* Any of state [6*npts], energy [nsteps+1], probes [(nsteps+1)*nprobes*6] may be NULL. */
+nwb_status nwb_pool_results(nwb_pool* p, int slot, double* state, double* energy, double* probes);
+nwb_status nwb_pool_remove(nwb_pool* p, int slot);
+nwb_status nwb_pool_info(const nwb_pool* p, size_t* used_bytes, size_t* budget_bytes,
+                         int* slots_used, long long* launches);
+/* Device time (ms, CUDA events on the pool's stream) of nsteps pool steps. */
+nwb_status nwb_pool_time_steps(nwb_pool* p, int nsteps, float* ms);
+nwb_status nwb_pool_destroy(nwb_pool* p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,23 @@ SIGNATURES = {
     "nwb_solver_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "nwb_solver_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_float), C.c_int]),
+    "nwb_pool_create": (C.c_int, [C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "nwb_pool_add": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.c_double, C.c_double, C.c_int,
+                               C.c_int, _I, _D, C.c_int, C.POINTER(C.c_int)]),
+    "nwb_pool_add_box": (C.c_int, [C.c_void_p] + [C.c_int] * 4 + [C.c_double] * 6 +
+                         [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _D, C.c_int,
+                          C.POINTER(C.c_int)]),
+    "nwb_pool_init_pulse": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "nwb_pool_upload": (C.c_int, [C.c_void_p, C.c_int, _D, C.c_size_t]),
+    "nwb_pool_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "nwb_pool_sync": (C.c_int, [C.c_void_p]),
+    "nwb_pool_query": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
+    "nwb_pool_results": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
+    "nwb_pool_remove": (C.c_int, [C.c_void_p, C.c_int]),
+    "nwb_pool_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                _I, C.POINTER(C.c_longlong)]),
+    "nwb_pool_time_steps": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    "nwb_pool_destroy": (C.c_int, [C.c_void_p]),
     "nwb_time_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int,
                                  C.POINTER(C.c_float)]),
     "nwb_time_stage_kernel": (C.c_int, [C.c_void_p, C.c_double, C.c_int,

@@ -1,0 +1,311 @@
+// batch.cu -- kernels of the multi-cavity pool: one persistent launch per LSRK
+// stage advances every resident cavity, whatever its N and element count.
+//
+// Blocks of kBatchThreads threads take tiles (EPB consecutive elements of one
+// cavity) from a work list through a per-stage atomic counter, largest tiles
+// first, and run the same fused stage tile as the single-mesh kernel
+// (stage_tile in stage_kernel.cuh) with the N-specialised shape of that tile.
+// A cavity's arithmetic does not depend on which other cavities share the
+// launch, so each result is bit-identical alone and in any mix.
+#include "batch.cuh"
+#include "stage_kernel.cuh"
+
+namespace nwb {
+namespace {
+
+using stage::SmemLayout;
+using stage::stage_tile;
+
+// Shape per N for 256-thread blocks: KS threads per column, EPB elements.
+template <int N> struct BShape;
+template <> struct BShape<2> { static constexpr int KS = 2, EPB = 32; };
+template <> struct BShape<3> { static constexpr int KS = 3, EPB = 9; };
+template <> struct BShape<4> { static constexpr int KS = 4, EPB = 4; };
+template <> struct BShape<5> { static constexpr int KS = 5, EPB = 2; };
+template <> struct BShape<6> { static constexpr int KS = 6, EPB = 1; };
+template <> struct BShape<7> { static constexpr int KS = 5, EPB = 1; };
+template <> struct BShape<8> { static constexpr int KS = 4, EPB = 1; };
+template <> struct BShape<9> { static constexpr int KS = 3, EPB = 1; };
+template <> struct BShape<10> { static constexpr int KS = 2, EPB = 1; };
+
+template <int N, bool F32>
+constexpr int bsmem() {
+    return SmemLayout<N, F32, BShape<N>::EPB, false>::total;
+}
+
+template <int N, bool F32>
+__device__ __forceinline__ void run_tile(const StageParams& P, int e0, unsigned char* smem, int tid) {
+    static_assert(BShape<N>::KS * BShape<N>::EPB * N * N <= kBatchThreads, "shape too large");
+    stage_tile<N, GEO_BOX, F32, BShape<N>::KS, BShape<N>::EPB, false>(P, e0, smem, tid);
+}
+
+// Carpenter-Kennedy LSRK45 (src/dg_solver.cpp:58-69).
+__constant__ double c_rk4a[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                                 -2404267990393.0 / 2016746695238.0,
+                                 -3550918686646.0 / 2091501179385.0,
+                                 -1275806237668.0 / 842570457699.0};
+__constant__ double c_rk4b[5] = {1432997174477.0 / 9575080441755.0,
+                                 5161836677717.0 / 13612068292357.0,
+                                 1720146321549.0 / 2090206949498.0,
+                                 3134564353537.0 / 4481467310338.0,
+                                 2277821191437.0 / 14882151754819.0};
+
+template <bool F32>
+__global__ void __launch_bounds__(kBatchThreads, 2)
+batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
+                   const int* __restrict__ ntiles_p, int* __restrict__ counters, int stage) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_tile;
+    const int tid = threadIdx.x;
+    const int ntiles = *ntiles_p;
+    for (;;) {
+        __syncthreads();  // the previous tile is done with shared memory
+        if (tid == 0) s_tile = atomicAdd(&counters[stage], 1);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= ntiles) break;
+        const WorkItem w = work[t];
+        const SlotDev& S = slots[w.slot];
+        if (!S.active) continue;
+        const int par = S.par ^ (stage & 1);
+        StageParams P;
+        P.u_in = S.u[par];
+        P.u_out = S.u[par ^ 1];
+        P.k = S.k;
+        P.stride = S.stride;
+        P.nelt = S.nelt;
+        P._pad0 = 0;
+        P.D = S.D;
+        P.geo = S.geo;
+        P.conn = S.conn;
+        P.met_n = nullptr;
+        P.fnrm = nullptr;
+        P.flift = nullptr;
+        P.fplus = nullptr;
+        P.nfp = 0;
+        P.c0 = S.c0;
+        P.a = c_rk4a[stage];
+        P.b = c_rk4b[stage];
+        P.dt = S.dt;
+        switch (w.N) {
+            case 2: run_tile<2, F32>(P, w.e0, smem, tid); break;
+            case 3: run_tile<3, F32>(P, w.e0, smem, tid); break;
+            case 4: run_tile<4, F32>(P, w.e0, smem, tid); break;
+            case 5: run_tile<5, F32>(P, w.e0, smem, tid); break;
+            case 6: run_tile<6, F32>(P, w.e0, smem, tid); break;
+            case 7: run_tile<7, F32>(P, w.e0, smem, tid); break;
+            case 8: run_tile<8, F32>(P, w.e0, smem, tid); break;
+            case 9: run_tile<9, F32>(P, w.e0, smem, tid); break;
+            case 10: run_tile<10, F32>(P, w.e0, smem, tid); break;
+            default: break;
+        }
+    }
+}
+
+// Does this slot record energy after the step it is taking now (post = 1), or
+// is this the initial-state record (post = 0)?
+__device__ __forceinline__ bool wants_energy(const SlotDev& S, int post) {
+    if (!post) return true;
+    const int next = S.done + 1;
+    return (next % S.energy_every) == 0 || next == S.nsteps;
+}
+
+// Energy partial of each tile, fixed order within the tile.
+__global__ void __launch_bounds__(256)
+batch_diag_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
+                  const int* __restrict__ ntiles_p, int post, int only_slot) {
+    const int ntiles = *ntiles_p;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = blockIdx.x * 8 + warp; t < ntiles; t += gridDim.x * 8) {
+        const WorkItem w = work[t];
+        if (only_slot >= 0 && w.slot != only_slot) continue;
+        const SlotDev& S = slots[w.slot];
+        if (!(S.active || !post) || !wants_energy(S, post)) continue;
+        const double* u = S.u[post ? (S.par ^ 1) : S.par];
+        const int N3 = S.N * S.N * S.N;
+        const int e1 = min(S.nelt, w.e0 + S.epb);
+        double acc = 0.0;
+        for (int e = w.e0; e < e1; ++e) {
+            const double J = S.geo[e].jdet;
+            const long long base = static_cast<long long>(e) * N3;
+            for (int m = lane; m < N3; m += 32) {
+                const long long p = base + m;
+                const long long st = S.stride;
+                const double ex = u[p], ey = u[st + p], ez = u[2 * st + p];
+                const double hx = u[3 * st + p], hy = u[4 * st + p], hz = u[5 * st + p];
+                acc += 0.5 * ((ex * ex + ey * ey + ez * ez) + (hx * hx + hy * hy + hz * hz)) *
+                       (J * S.w3[m]);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (lane == 0) S.partial[w.tile] = acc;
+    }
+}
+
+// One block per slot: warp 0 sums the energy partials in a fixed order, warps
+// 1..kMaxProbes evaluate the probes (tensor-product Lagrange interpolation of
+// the element's nodes, as ProbeManager::record does on the host,
+// src/probe.cpp:192-216), then thread 0 advances the slot's step bookkeeping.
+__global__ void __launch_bounds__(32 * (kMaxProbes + 1))
+batch_epilogue_kernel(SlotDev* __restrict__ slots, int nslots, int post, int only_slot,
+                      int* __restrict__ counters) {
+    if (blockIdx.x == 0 && threadIdx.x < 8 && post) counters[threadIdx.x] = 0;
+    const int s = blockIdx.x;
+    if (s >= nslots || (only_slot >= 0 && s != only_slot)) return;
+    SlotDev& S = slots[s];
+    if (post && !S.active) return;
+    if (!post && !S.u[0]) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int idx = post ? S.done + 1 : 0;  // history index written by this call
+    const double* u = S.u[post ? (S.par ^ 1) : S.par];
+    if (warp == 0 && wants_energy(S, post)) {
+        double acc = 0.0;
+        for (int t = lane; t < S.ntiles; t += 32) acc += S.partial[t];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (lane == 0) S.energy[idx] = acc;
+    } else if (warp == 0 && lane == 0) {
+        S.energy[idx] = __longlong_as_double(0x7ff8000000000000LL);  // not recorded this step
+    }
+    if (warp >= 1 && warp - 1 < S.nprobes) {
+        const int pr = warp - 1;
+        const int N = S.N, N2 = N * N, N3 = N2 * N;
+        const double* wr = S.probe_w + pr * 3 * N;
+        const double* ws = wr + N;
+        const double* wt = ws + N;
+        const long long base = static_cast<long long>(S.probe_elem[pr]) * N3;
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int m = lane; m < N3; m += 32) {
+            const int i = m % N, j = (m / N) % N, k = m / N2;
+            const double wgt = wr[i] * ws[j] * wt[k];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc[c] += wgt * u[c * S.stride + base + m];
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], off);
+        }
+        if (lane == 0) {
+            double* out = S.probes + (static_cast<long long>(idx) * S.nprobes + pr) * 6;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) out[c] = acc[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && post) {
+        S.par ^= 1;
+        S.done += 1;
+        if (S.done >= S.nsteps) S.active = 0;
+    }
+}
+
+__global__ void box_pulse_kernel(const BoxPulse b, double* __restrict__ u, long long stride) {
+    const int N = b.N, N3 = N * N * N;
+    const long long npts = static_cast<long long>(b.nel[0]) * b.nel[1] * b.nel[2] * N3;
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < npts;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long e = p / N3;
+        const int m = static_cast<int>(p - e * N3);
+        const int i = m % N, j = (m / N) % N, k = m / (N * N);
+        const int ex = static_cast<int>(e % b.nel[0]);
+        const int ey = static_cast<int>((e / b.nel[0]) % b.nel[1]);
+        const int ez = static_cast<int>(e / (static_cast<long long>(b.nel[0]) * b.nel[1]));
+        const double x = b.lo[0] + (ex + 0.5 * (b.z[i] + 1.0)) * b.h[0];
+        const double y = b.lo[1] + (ey + 0.5 * (b.z[j] + 1.0)) * b.h[1];
+        const double z = b.lo[2] + (ez + 0.5 * (b.z[k] + 1.0)) * b.h[2];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double* q = b.pulse + 5 * c;
+            double v = 0.0;
+            if (q[4] > 0.0) {
+                const double dx = x - q[1], dy = y - q[2], dz = z - q[3];
+                v = q[0] * exp(-(dx * dx + dy * dy + dz * dz) / (q[4] * q[4]));
+            }
+            u[c * stride + p] = v;
+        }
+    }
+}
+
+template <bool F32>
+int max_batch_smem() {
+    int m = 0;
+    m = max(m, bsmem<2, F32>()); m = max(m, bsmem<3, F32>()); m = max(m, bsmem<4, F32>());
+    m = max(m, bsmem<5, F32>()); m = max(m, bsmem<6, F32>()); m = max(m, bsmem<7, F32>());
+    m = max(m, bsmem<8, F32>()); m = max(m, bsmem<9, F32>()); m = max(m, bsmem<10, F32>());
+    return m;
+}
+
+}  // namespace
+
+BatchShape batch_shape(int N, int f32) {
+    (void)f32;
+    switch (N) {
+        case 2: return {BShape<2>::KS, BShape<2>::EPB};
+        case 3: return {BShape<3>::KS, BShape<3>::EPB};
+        case 4: return {BShape<4>::KS, BShape<4>::EPB};
+        case 5: return {BShape<5>::KS, BShape<5>::EPB};
+        case 6: return {BShape<6>::KS, BShape<6>::EPB};
+        case 7: return {BShape<7>::KS, BShape<7>::EPB};
+        case 8: return {BShape<8>::KS, BShape<8>::EPB};
+        case 9: return {BShape<9>::KS, BShape<9>::EPB};
+        case 10: return {BShape<10>::KS, BShape<10>::EPB};
+        default: return {0, 0};
+    }
+}
+
+int batch_smem(int N, int f32) {
+    switch (N) {
+        case 2: return f32 ? bsmem<2, true>() : bsmem<2, false>();
+        case 3: return f32 ? bsmem<3, true>() : bsmem<3, false>();
+        case 4: return f32 ? bsmem<4, true>() : bsmem<4, false>();
+        case 5: return f32 ? bsmem<5, true>() : bsmem<5, false>();
+        case 6: return f32 ? bsmem<6, true>() : bsmem<6, false>();
+        case 7: return f32 ? bsmem<7, true>() : bsmem<7, false>();
+        case 8: return f32 ? bsmem<8, true>() : bsmem<8, false>();
+        case 9: return f32 ? bsmem<9, true>() : bsmem<9, false>();
+        case 10: return f32 ? bsmem<10, true>() : bsmem<10, false>();
+        default: return 0;
+    }
+}
+
+cudaError_t batch_prepare(int f32, int smem) {
+    const int cap = f32 ? max_batch_smem<true>() : max_batch_smem<false>();
+    if (smem > cap) smem = cap;
+    return f32 ? cudaFuncSetAttribute(batch_stage_kernel<true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, cap)
+               : cudaFuncSetAttribute(batch_stage_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
+cudaError_t launch_batch_stage(int f32, int stage, const SlotDev* slots, const WorkItem* work,
+                               const int* ntiles, int* counters, int grid, int smem,
+                               cudaStream_t st) {
+    if (f32)
+        batch_stage_kernel<true><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage);
+    else
+        batch_stage_kernel<false><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_box_pulse(const BoxPulse& b, double* u, long long stride, cudaStream_t st) {
+    box_pulse_kernel<<<148 * 8, 256, 0, st>>>(b, u, stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_diag(SlotDev* slots, const WorkItem* work, const int* ntiles, int post,
+                              int only_slot, int grid, cudaStream_t st) {
+    batch_diag_kernel<<<grid, 256, 0, st>>>(slots, work, ntiles, post, only_slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_epilogue(SlotDev* slots, int nslots, int post, int only_slot,
+                                  int* counters, cudaStream_t st) {
+    if (nslots < 1) return cudaSuccess;
+    batch_epilogue_kernel<<<nslots, 32 * (kMaxProbes + 1), 0, st>>>(slots, nslots, post, only_slot,
+                                                                  counters);
+    return cudaGetLastError();
+}
+
+}  // namespace nwb

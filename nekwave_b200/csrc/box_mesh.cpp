@@ -46,6 +46,10 @@ double legendre_deriv(int n, double x) {
     return (n / (x * x - 1.0)) * (x * legendre(n, x) - legendre(n - 1, x));
 }
 
+}  // namespace
+
+namespace nwb {
+
 // GLL nodes, weights and the collocation derivative matrix (column-major
 // D[i + j N] = l_j'(x_i)): Newton on L'_p from a Chebyshev start, weights
 // 2/(p(p+1)L_p^2), corner entries -+p(p+1)/4 (src/mesh.cpp:64-145).
@@ -83,6 +87,59 @@ void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<doub
             D[i + j * N] = v;
         }
 }
+
+// Trilinear map of one element with the reference's operation order
+// (src/mesh.cpp:188-314): position, J and J^{-T} (rx,sx,tx,ry,sy,ty,rz,sz,tz)
+// at reference point (r,s,t).
+void trilinear_point(const double c[8][3], double r, double s, double t, double* X, double* J,
+                     double met[9]) {
+    const double Nf[8] = {
+        0.125 * (1.0 - r) * (1.0 - s) * (1.0 - t), 0.125 * (1.0 + r) * (1.0 - s) * (1.0 - t),
+        0.125 * (1.0 + r) * (1.0 + s) * (1.0 - t), 0.125 * (1.0 - r) * (1.0 + s) * (1.0 - t),
+        0.125 * (1.0 - r) * (1.0 - s) * (1.0 + t), 0.125 * (1.0 + r) * (1.0 - s) * (1.0 + t),
+        0.125 * (1.0 + r) * (1.0 + s) * (1.0 + t), 0.125 * (1.0 - r) * (1.0 + s) * (1.0 + t)};
+    const double dr[8] = {
+        -0.125 * (1.0 - s) * (1.0 - t), 0.125 * (1.0 - s) * (1.0 - t),
+        0.125 * (1.0 + s) * (1.0 - t), -0.125 * (1.0 + s) * (1.0 - t),
+        -0.125 * (1.0 - s) * (1.0 + t), 0.125 * (1.0 - s) * (1.0 + t),
+        0.125 * (1.0 + s) * (1.0 + t), -0.125 * (1.0 + s) * (1.0 + t)};
+    const double ds[8] = {
+        -0.125 * (1.0 - r) * (1.0 - t), -0.125 * (1.0 + r) * (1.0 - t),
+        0.125 * (1.0 + r) * (1.0 - t), 0.125 * (1.0 - r) * (1.0 - t),
+        -0.125 * (1.0 - r) * (1.0 + t), -0.125 * (1.0 + r) * (1.0 + t),
+        0.125 * (1.0 + r) * (1.0 + t), 0.125 * (1.0 - r) * (1.0 + t)};
+    const double dt[8] = {
+        -0.125 * (1.0 - r) * (1.0 - s), -0.125 * (1.0 + r) * (1.0 - s),
+        -0.125 * (1.0 + r) * (1.0 + s), -0.125 * (1.0 - r) * (1.0 + s),
+        0.125 * (1.0 - r) * (1.0 - s), 0.125 * (1.0 + r) * (1.0 - s),
+        0.125 * (1.0 + r) * (1.0 + s), 0.125 * (1.0 - r) * (1.0 + s)};
+    double px = 0, py = 0, pz = 0, xr = 0, yr = 0, zr = 0, xs = 0, ys = 0, zs = 0, xt = 0, yt = 0, zt = 0;
+    for (int a = 0; a < 8; ++a) {
+        const double vx = c[a][0], vy = c[a][1], vz = c[a][2];
+        px += Nf[a] * vx; py += Nf[a] * vy; pz += Nf[a] * vz;
+        xr += dr[a] * vx; yr += dr[a] * vy; zr += dr[a] * vz;
+        xs += ds[a] * vx; ys += ds[a] * vy; zs += ds[a] * vz;
+        xt += dt[a] * vx; yt += dt[a] * vy; zt += dt[a] * vz;
+    }
+    if (X) { X[0] = px; X[1] = py; X[2] = pz; }
+    const double detJ = xr * (ys * zt - yt * zs) - xs * (yr * zt - yt * zr) + xt * (yr * zs - ys * zr);
+    *J = detJ;
+    const double invJ = 1.0 / detJ;
+    met[0] = invJ * (ys * zt - yt * zs);
+    met[1] = invJ * (yt * zr - yr * zt);
+    met[2] = invJ * (yr * zs - ys * zr);
+    met[3] = invJ * (xt * zs - xs * zt);
+    met[4] = invJ * (xr * zt - xt * zr);
+    met[5] = invJ * (xs * zr - xr * zs);
+    met[6] = invJ * (xs * yt - xt * ys);
+    met[7] = invJ * (xt * yr - xr * yt);
+    met[8] = invJ * (xr * ys - xs * yr);
+}
+
+}  // namespace nwb
+
+namespace {
+using nwb::gll;
 
 inline int face_node(int N, int e, int f, int p, int q) {
     int i = 0, j = 0, k = 0;

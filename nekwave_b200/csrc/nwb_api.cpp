@@ -73,15 +73,21 @@ inline void orient(int N, int o, int p, int q, int* pp, int* qq) {
     *qq = b;
 }
 
-// Host-side result of the mesh analysis.
-struct Analysis {
-    int geo = nwb::GEO_NODAL;
-    std::vector<nwb::ElemGeo> egeo;
-    std::vector<int> conn;
-    std::vector<double> jac_e;
-};
+}  // namespace
 
-nwb_status analyse(const nwb_mesh_desc* m, Analysis* A) {
+namespace nwb {
+
+nwb_status set_error(nwb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A) {
     const int N = m->N, nelt = m->nelt, N2 = N * N, N3 = N2 * N;
     const long long npts = static_cast<long long>(nelt) * N3;
     // canonical face-point order (src/mesh.cpp:1003-1004) is part of the contract
@@ -170,6 +176,11 @@ nwb_status analyse(const nwb_mesh_desc* m, Analysis* A) {
     }
     return NWB_OK;
 }
+
+}  // namespace nwb
+
+namespace {
+using nwb::Analysis;
 
 template <class T>
 nwb_status dalloc(T** p, size_t count, size_t* total) {
@@ -375,7 +386,7 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
 
     Analysis A;
     try {
-        nwb_status r = analyse(m, &A);
+        nwb_status r = nwb::analyse_mesh(m, &A);
         if (r != NWB_OK) return r;
     } catch (const std::bad_alloc&) {
         return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");

@@ -63,6 +63,24 @@ struct StageConfig {
     int minb;     // minimum resident blocks requested from the register allocator
 };
 
+}  // namespace nwb
+
+#include <vector>
+#include "nwb.h"
+
+namespace nwb {
+
+// Host-side result of the mesh analysis (nwb_api.cpp): geometry class and, for
+// the affine classes, the compressed per-element geometry and connections.
+struct Analysis {
+    int geo = GEO_NODAL;
+    std::vector<ElemGeo> egeo;
+    std::vector<int> conn;
+    std::vector<double> jac_e;
+};
+nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A);
+nwb_status set_error(nwb_status s, const char* fmt, ...);
+
 // Fused stage kernel (stage_inst.cu, one object per N).  Variant 0 exists for
 // every (N, geometry, precision); the axis-aligned class has more variants,
 // which the autotuner times.  Returns cudaErrorInvalidValue for an unknown

@@ -1,0 +1,728 @@
+// pool.cpp -- many independent cavities resident on one GPU, advanced together.
+//
+// The reference solves one mesh per process (Case::simulate, src/case.cpp:529-660).
+// A pool keeps many cavities ("slots") resident in HBM at once and advances all
+// active ones with one persistent launch per LSRK stage (batch.cu):
+//   * admission by a fixed HBM budget: the pool owns one arena allocated at
+//     creation and sub-allocates every slot's buffers from it, so admitting a
+//     cavity never calls cudaMalloc and fails with NWB_EBUSY when it does not fit;
+//   * a step of all slots is one CUDA graph (5 stage launches, diagnostics,
+//     step epilogue) replayed as often as needed; slots that have taken their
+//     steps fall idle on the device, and slots can be added or removed between
+//     replays (the graph reads the slot table and the work list from device
+//     memory, so it stays valid);
+//   * per-slot energy history and probe traces are recorded on the device.
+#include "batch.cuh"
+#include "nwb.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+namespace nwb {
+void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<double>& D);
+void trilinear_point(const double c[8][3], double r, double s, double t, double* X, double* J,
+                     double met[9]);
+}  // namespace nwb
+
+namespace {
+
+using nwb::set_error;
+
+#define NWB_PCU(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return set_error(NWB_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                             __LINE__);                                                       \
+    } while (0)
+
+constexpr size_t kAlign = 256;
+
+struct Range {
+    size_t off, size;
+};
+
+// First-fit sub-allocator over the arena; frees coalesce with their neighbours.
+class Arena {
+public:
+    void reset(size_t bytes) {
+        free_.clear();
+        free_[0] = bytes;
+        total_ = bytes;
+        used_ = 0;
+    }
+    bool alloc(size_t bytes, Range* r) {
+        bytes = (std::max<size_t>(bytes, 1) + kAlign - 1) / kAlign * kAlign;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                r->off = it->first;
+                r->size = bytes;
+                const size_t rest = it->second - bytes;
+                const size_t noff = it->first + bytes;
+                free_.erase(it);
+                if (rest) free_[noff] = rest;
+                used_ += bytes;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(const Range& r) {
+        used_ -= r.size;
+        auto it = free_.emplace(r.off, r.size).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    size_t used() const { return used_; }
+    size_t total() const { return total_; }
+
+private:
+    std::map<size_t, size_t> free_;
+    size_t total_ = 0, used_ = 0;
+};
+
+struct SlotHost {
+    bool used = false;
+    bool uploaded = false;
+    bool is_box = false;
+    nwb::BoxPulse box{};
+    int N = 0, nelt = 0, nsteps = 0, nprobes = 0, energy_every = 1, ntiles = 0, epb = 1;
+    long long npts = 0, stride = 0;
+    std::vector<Range> ranges;
+    nwb::SlotDev dev{};
+};
+
+}  // namespace
+
+struct nwb_pool {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    int f32 = 0;
+    char* base = nullptr;
+    Arena arena;
+    int max_slots = 0;
+    std::vector<SlotHost> slots;
+    nwb::SlotDev* d_slots = nullptr;
+    nwb::WorkItem* d_work = nullptr;
+    int work_cap = 0;
+    int* d_ntiles = nullptr;
+    int* d_counters = nullptr;
+    bool work_dirty = true;
+    int ntiles = 0;
+    int smem_needed = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_smem = -1;
+    int grid = 0, diag_grid = 0;
+    int sms = 148;
+    long long launches = 0;
+
+    template <class T>
+    T* ptr(const Range& r) const {
+        return reinterpret_cast<T*>(base + r.off);
+    }
+
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_smem = -1;
+    }
+
+    nwb_status write_slot(int s) {
+        NWB_PCU(cudaMemcpyAsync(d_slots + s, &slots[s].dev, sizeof(nwb::SlotDev),
+                                cudaMemcpyHostToDevice, st));
+        // the host copy is a member of a live vector and may change before the
+        // copy runs: wait for it here (slot changes are rare, between replays)
+        NWB_PCU(cudaStreamSynchronize(st));
+        return NWB_OK;
+    }
+
+    // Work list: every tile of every used slot, largest tiles first, so the
+    // dynamic tile counter hands out the long tiles early.
+    nwb_status rebuild_work() {
+        if (!work_dirty) return NWB_OK;
+        std::vector<nwb::WorkItem> w;
+        smem_needed = 0;
+        for (int s = 0; s < max_slots; ++s) {
+            const SlotHost& h = slots[s];
+            if (!h.used) continue;
+            smem_needed = std::max(smem_needed, nwb::batch_smem(h.N, f32));
+            for (int t = 0; t < h.ntiles; ++t) w.push_back(nwb::WorkItem{s, t * h.epb, h.N, t});
+        }
+        std::stable_sort(w.begin(), w.end(), [&](const nwb::WorkItem& a, const nwb::WorkItem& b) {
+            const long long ca = static_cast<long long>(slots[a.slot].epb) * a.N * a.N * a.N;
+            const long long cb = static_cast<long long>(slots[b.slot].epb) * b.N * b.N * b.N;
+            return ca > cb;
+        });
+        ntiles = static_cast<int>(w.size());
+        if (ntiles > work_cap) {
+            if (d_work) cudaFree(d_work);
+            d_work = nullptr;
+            work_cap = std::max(ntiles, 2 * work_cap);
+            drop_graph();
+            NWB_PCU(cudaMalloc(&d_work, sizeof(nwb::WorkItem) * work_cap));
+        }
+        if (ntiles)
+            NWB_PCU(cudaMemcpyAsync(d_work, w.data(), sizeof(nwb::WorkItem) * ntiles,
+                                    cudaMemcpyHostToDevice, st));
+        NWB_PCU(cudaMemcpyAsync(d_ntiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, st));
+        NWB_PCU(cudaStreamSynchronize(st));
+        work_dirty = false;
+        return NWB_OK;
+    }
+
+    nwb_status launch_step() {
+        for (int s = 0; s < 5; ++s) {
+            cudaError_t e = nwb::launch_batch_stage(f32, s, d_slots, d_work, d_ntiles, d_counters,
+                                                    grid, graph_smem, st);
+            if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch stage: %s", cudaGetErrorString(e));
+        }
+        cudaError_t e = nwb::launch_batch_diag(d_slots, d_work, d_ntiles, 1, -1, diag_grid, st);
+        if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch diag: %s", cudaGetErrorString(e));
+        e = nwb::launch_batch_epilogue(d_slots, max_slots, 1, -1, d_counters, st);
+        if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch epilogue: %s", cudaGetErrorString(e));
+        return NWB_OK;
+    }
+
+    nwb_status ensure_graph() {
+        nwb_status r = rebuild_work();
+        if (r != NWB_OK) return r;
+        const int want = std::max(smem_needed, 1024);
+        if (graph && graph_smem >= want) return NWB_OK;
+        drop_graph();
+        graph_smem = want;
+        NWB_PCU(nwb::batch_prepare(f32, graph_smem));
+        // persistent grid: as many resident blocks as the shared memory allows
+        const int by_smem = std::max(1, (227 * 1024) / (graph_smem + 1024));
+        grid = sms * std::min(2, by_smem);
+        diag_grid = sms * 4;
+        cudaGraph_t g = nullptr;
+        NWB_PCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        r = launch_step();
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (r != NWB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "instantiate: %s", cudaGetErrorString(ce));
+        return NWB_OK;
+    }
+
+    void release_slot(int s) {
+        for (const Range& r : slots[s].ranges) arena.release(r);
+        slots[s] = SlotHost{};
+    }
+};
+
+extern "C" {
+
+nwb_status nwb_pool_create(size_t hbm_budget_bytes, int max_slots, nwb_precision prec,
+                           nwb_pool** out) {
+    if (!out) return set_error(NWB_EINVAL, "nwb_pool_create: out is null");
+    *out = nullptr;
+    if (max_slots < 1 || max_slots > 65536 || hbm_budget_bytes < (1u << 20))
+        return set_error(NWB_EINVAL, "nwb_pool_create: need 1..65536 slots and >= 1 MiB budget");
+    if (prec != NWB_FP64 && prec != NWB_FP32_BULK)
+        return set_error(NWB_EINVAL, "nwb_pool_create: unknown precision");
+    nwb_pool* p = new (std::nothrow) nwb_pool();
+    if (!p) return set_error(NWB_ENOMEM, "nwb_pool_create: out of host memory");
+    p->f32 = prec == NWB_FP32_BULK;
+    p->max_slots = max_slots;
+    p->slots.resize(max_slots);
+    auto bail = [&](nwb_status r) {
+        nwb_pool_destroy(p);
+        return r;
+    };
+    cudaError_t e = cudaGetDevice(&p->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(set_error(NWB_ECUDA, "nwb_pool_create: %s", cudaGetErrorString(e)));
+    e = cudaMalloc(&p->base, hbm_budget_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bail(set_error(NWB_ENOMEM, "nwb_pool_create: arena of %zu bytes: %s", hbm_budget_bytes,
+                              cudaGetErrorString(e)));
+    }
+    p->arena.reset(hbm_budget_bytes);
+    e = cudaMalloc(&p->d_slots, sizeof(nwb::SlotDev) * max_slots);
+    if (e == cudaSuccess) e = cudaMemset(p->d_slots, 0, sizeof(nwb::SlotDev) * max_slots);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_ntiles, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->d_ntiles, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_counters, sizeof(int) * 8);
+    if (e == cudaSuccess) e = cudaMemset(p->d_counters, 0, sizeof(int) * 8);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return bail(set_error(NWB_ECUDA, "nwb_pool_create: %s", cudaGetErrorString(e)));
+    *out = p;
+    return NWB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Admits one cavity given its compressed axis-aligned geometry.
+nwb_status admit(nwb_pool* p, int N, int nelt, const double* D, const double* w3,
+                 const nwb::ElemGeo* egeo, const int* conn, double c0, double dt, int nsteps,
+                 int nprobes, const int* probe_elem, const double* probe_w, int energy_every,
+                 int* slot_out, SlotHost** host_out) {
+    int s = -1;
+    for (int i = 0; i < p->max_slots; ++i)
+        if (!p->slots[i].used) {
+            s = i;
+            break;
+        }
+    if (s < 0) return set_error(NWB_EBUSY, "nwb_pool_add: all %d slots busy", p->max_slots);
+    const int N2 = N * N, N3 = N2 * N;
+    const nwb::BatchShape sh = nwb::batch_shape(N, p->f32);
+    SlotHost h;
+    h.used = true;
+    h.N = N;
+    h.nelt = nelt;
+    h.nsteps = nsteps;
+    h.nprobes = nprobes;
+    h.energy_every = energy_every;
+    h.epb = sh.epb;
+    h.ntiles = (nelt + sh.epb - 1) / sh.epb;
+    h.npts = static_cast<long long>(nelt) * N3;
+    h.stride = (h.npts + 63) / 64 * 64;
+    // buffers, in one list so a failed admission releases what it took
+    const size_t sizes[] = {
+        sizeof(double) * 6 * static_cast<size_t>(h.stride),                 // 0 u0
+        sizeof(double) * 6 * static_cast<size_t>(h.stride),                 // 1 u1
+        sizeof(double) * 6 * static_cast<size_t>(h.stride),                 // 2 k
+        sizeof(double) * N2,                                                // 3 D
+        sizeof(double) * N3,                                                // 4 w3
+        sizeof(nwb::ElemGeo) * nelt,                                        // 5 geo
+        sizeof(int) * 6 * static_cast<size_t>(nelt),                        // 6 conn
+        sizeof(double) * h.ntiles,                                          // 7 partial
+        sizeof(double) * (nsteps + 1),                                      // 8 energy
+        sizeof(double) * 6 * static_cast<size_t>(nprobes) * (nsteps + 1),   // 9 probes
+        sizeof(int) * std::max(nprobes, 1),                                 // 10 probe elements
+        sizeof(double) * 3 * N * std::max(nprobes, 1)};                     // 11 probe weights
+    for (size_t b : sizes) {
+        Range r;
+        if (!p->arena.alloc(b, &r)) {
+            for (const Range& q : h.ranges) p->arena.release(q);
+            return set_error(NWB_EBUSY, "nwb_pool_add: over the HBM budget (%zu of %zu bytes in use)",
+                             p->arena.used(), p->arena.total());
+        }
+        h.ranges.push_back(r);
+    }
+    nwb::SlotDev& d = h.dev;
+    d.u[0] = p->ptr<double>(h.ranges[0]);
+    d.u[1] = p->ptr<double>(h.ranges[1]);
+    d.k = p->ptr<double>(h.ranges[2]);
+    d.D = p->ptr<double>(h.ranges[3]);
+    d.w3 = p->ptr<double>(h.ranges[4]);
+    d.geo = p->ptr<nwb::ElemGeo>(h.ranges[5]);
+    d.conn = p->ptr<int>(h.ranges[6]);
+    d.partial = p->ptr<double>(h.ranges[7]);
+    d.energy = p->ptr<double>(h.ranges[8]);
+    d.probes = p->ptr<double>(h.ranges[9]);
+    d.probe_elem = p->ptr<int>(h.ranges[10]);
+    d.probe_w = p->ptr<double>(h.ranges[11]);
+    d.stride = h.stride;
+    d.c0 = c0;
+    d.dt = dt;
+    d.N = N;
+    d.nelt = nelt;
+    d.ntiles = h.ntiles;
+    d.epb = h.epb;
+    d.nprobes = nprobes;
+    d.energy_every = energy_every;
+    d.nsteps = nsteps;
+    d.done = 0;
+    d.par = 0;
+    d.active = 0;  // set when the initial state arrives
+    auto cp = [&](int idx, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpyAsync(p->base + h.ranges[idx].off, src, bytes, cudaMemcpyHostToDevice, p->st)
+                     : cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < 3 && e == cudaSuccess; ++b)
+        e = cudaMemsetAsync(p->base + h.ranges[b].off, 0, sizes[b], p->st);
+    if (e == cudaSuccess) e = cp(3, D, sizes[3]);
+    if (e == cudaSuccess) e = cp(4, w3, sizes[4]);
+    if (e == cudaSuccess) e = cp(5, egeo, sizes[5]);
+    if (e == cudaSuccess) e = cp(6, conn, sizes[6]);
+    if (e == cudaSuccess && nprobes) e = cp(10, probe_elem, sizeof(int) * nprobes);
+    if (e == cudaSuccess && nprobes) e = cp(11, probe_w, sizeof(double) * 3 * N * nprobes);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->st);
+    if (e != cudaSuccess) {
+        for (const Range& q : h.ranges) p->arena.release(q);
+        return set_error(NWB_ECUDA, "nwb_pool_add: %s", cudaGetErrorString(e));
+    }
+    p->slots[s] = h;
+    nwb_status r = p->write_slot(s);
+    if (r != NWB_OK) {
+        p->release_slot(s);
+        return r;
+    }
+    p->work_dirty = true;
+    *slot_out = s;
+    if (host_out) *host_out = &p->slots[s];
+    return NWB_OK;
+}
+
+// Per-element geometry of a box cavity, computed from the box parameters with
+// the reference's trilinear arithmetic at exactly the nodes the mesh analysis
+// samples (node 0 for J^{-T} and J, face point (0,0) for each face's normal and
+// lift), so it equals what nwb_box_mesh_create + analysis would produce.
+void box_geometry(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                  int pmask, const std::vector<double>& z, const std::vector<double>& w,
+                  std::vector<nwb::ElemGeo>& geo, std::vector<int>& conn) {
+    const int nelt = nelx * nely * nelz;
+    geo.assign(nelt, nwb::ElemGeo{});
+    conn.assign(6 * static_cast<size_t>(nelt), nwb::kConnPEC);
+    const double dx = (hi[0] - lo[0]) / nelx, dy = (hi[1] - lo[1]) / nely, dz = (hi[2] - lo[2]) / nelz;
+    const int last = N - 1;
+    // local (i,j,k) of face point (0,0) of faces 0..5 (src/mesh.cpp:959-976)
+    const int fi[6][3] = {{0, 0, 0}, {last, 0, 0}, {0, last, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, last}};
+    const double sgn[6] = {-1, 1, 1, -1, -1, 1};
+    const int row[6] = {1, 0, 1, 0, 2, 2};  // s, r, s, r, t, t
+    auto eidx = [=](int a, int b, int c) { return a + nelx * (b + nely * c); };
+    for (int ez = 0; ez < nelz; ++ez)
+        for (int ey = 0; ey < nely; ++ey)
+            for (int ex = 0; ex < nelx; ++ex) {
+                const double x0 = lo[0] + ex * dx, x1 = x0 + dx;
+                const double y0 = lo[1] + ey * dy, y1 = y0 + dy;
+                const double z0 = lo[2] + ez * dz, z1 = z0 + dz;
+                const double c[8][3] = {{x0, y0, z0}, {x1, y0, z0}, {x1, y1, z0}, {x0, y1, z0},
+                                        {x0, y0, z1}, {x1, y0, z1}, {x1, y1, z1}, {x0, y1, z1}};
+                const int e = eidx(ex, ey, ez);
+                nwb::ElemGeo& G = geo[e];
+                double J0;
+                nwb::trilinear_point(c, z[0], z[0], z[0], nullptr, &J0, G.met);
+                G.jdet = J0;
+                for (int f = 0; f < 6; ++f) {
+                    double J, met[9];
+                    nwb::trilinear_point(c, z[fi[f][0]], z[fi[f][1]], z[fi[f][2]], nullptr, &J, met);
+                    // row of J^{-T} for the face's reference direction: (r|s|t)_(x,y,z)
+                    const double Nx = sgn[f] * J * met[row[f] + 0];
+                    const double Ny = sgn[f] * J * met[row[f] + 3];
+                    const double Nz = sgn[f] * J * met[row[f] + 6];
+                    const double L = std::sqrt(Nx * Nx + Ny * Ny + Nz * Nz);
+                    G.nrm[f][0] = (L > 1e-14) ? (Nx / L) : 0.0;
+                    G.nrm[f][1] = (L > 1e-14) ? (Ny / L) : 0.0;
+                    G.nrm[f][2] = (L > 1e-14) ? (Nz / L) : 0.0;
+                    const double dA = L * (w[0] * w[0]);
+                    const double w3v = w[fi[f][0]] * w[fi[f][1]] * w[fi[f][2]];
+                    G.lift[f] = dA / (J * w3v);
+                }
+                int nb[6];
+                nb[0] = ey > 0 ? eidx(ex, ey - 1, ez) : ((pmask & 2) ? eidx(ex, nely - 1, ez) : -1);
+                nb[1] = ex < nelx - 1 ? eidx(ex + 1, ey, ez) : ((pmask & 1) ? eidx(0, ey, ez) : -1);
+                nb[2] = ey < nely - 1 ? eidx(ex, ey + 1, ez) : ((pmask & 2) ? eidx(ex, 0, ez) : -1);
+                nb[3] = ex > 0 ? eidx(ex - 1, ey, ez) : ((pmask & 1) ? eidx(nelx - 1, ey, ez) : -1);
+                nb[4] = ez > 0 ? eidx(ex, ey, ez - 1) : ((pmask & 4) ? eidx(ex, ey, nelz - 1) : -1);
+                nb[5] = ez < nelz - 1 ? eidx(ex, ey, ez + 1) : ((pmask & 4) ? eidx(ex, ey, 0) : -1);
+                const int opp[6] = {2, 3, 0, 1, 5, 4};
+                for (int f = 0; f < 6; ++f)
+                    conn[6 * static_cast<size_t>(e) + f] = nb[f] < 0 ? nwb::kConnPEC : ((nb[f] << 6) | (opp[f] << 3));
+            }
+}
+
+// ProbeManager::init (src/probe.cpp:33-96) on a box: first element whose box is
+// nearest, reference coordinates clamped to [-1,1], tensor Lagrange weights
+// (src/probe.cpp:11-30).
+void box_probes(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                const std::vector<double>& z, int nprobes, const double* xyz, std::vector<int>& elem,
+                std::vector<double>& wts) {
+    const double h[3] = {(hi[0] - lo[0]) / nelx, (hi[1] - lo[1]) / nely, (hi[2] - lo[2]) / nelz};
+    const int nel[3] = {nelx, nely, nelz};
+    elem.assign(nprobes, 0);
+    wts.assign(static_cast<size_t>(nprobes) * 3 * N, 0.0);
+    for (int q = 0; q < nprobes; ++q) {
+        // the nearest element per axis, lowest index on ties (argmin over e)
+        int best[3];
+        double ref[3];
+        for (int a = 0; a < 3; ++a) {
+            double bd = 1e300;
+            int bi = 0;
+            double br = 0;
+            for (int i = 0; i < nel[a]; ++i) {
+                const double x0 = lo[a] + i * h[a], x1 = x0 + h[a];
+                const double r = std::abs(x1 - x0) > 1e-14 ? 2.0 * (xyz[3 * q + a] - x0) / (x1 - x0) - 1.0 : 0.0;
+                const double d = std::max(0.0, std::max(-1.0 - r, r - 1.0));
+                if (d * d < bd) {
+                    bd = d * d;
+                    bi = i;
+                    br = std::max(-1.0, std::min(1.0, r));
+                }
+            }
+            best[a] = bi;
+            ref[a] = br;
+        }
+        elem[q] = best[0] + nelx * (best[1] + nely * best[2]);
+        for (int a = 0; a < 3; ++a) {
+            double* L = &wts[(static_cast<size_t>(q) * 3 + a) * N];
+            int hit = -1;
+            for (int i = 0; i < N; ++i)
+                if (std::abs(ref[a] - z[i]) < 1e-12) { hit = i; break; }
+            for (int i = 0; i < N; ++i) L[i] = hit >= 0 ? (i == hit ? 1.0 : 0.0) : 1.0;
+            if (hit >= 0) continue;
+            for (int i = 0; i < N; ++i)
+                for (int j = 0; j < N; ++j)
+                    if (i != j) L[i] *= (ref[a] - z[j]) / (z[i] - z[j]);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+nwb_status nwb_pool_add(nwb_pool* p, const nwb_mesh_desc* m, double c0, double dt, int nsteps,
+                        int nprobes, const int* probe_elem, const double* probe_w,
+                        int energy_every, int* slot_out) {
+    if (!p || !m || !slot_out) return set_error(NWB_EINVAL, "nwb_pool_add: null argument");
+    if (m->N < 2 || m->N > 10 || m->nelt < 1 || nsteps < 1 || !std::isfinite(dt) || dt <= 0 ||
+        nprobes < 0 || nprobes > nwb::kMaxProbes || energy_every < 1 ||
+        (nprobes > 0 && (!probe_elem || !probe_w)))
+        return set_error(NWB_EINVAL, "nwb_pool_add: bad arguments (N 2..10, nsteps >= 1, dt > 0, "
+                                     "0..8 probes, energy_every >= 1)");
+    nwb::Analysis A;
+    try {
+        nwb_status r = nwb::analyse_mesh(m, &A);
+        if (r != NWB_OK) return r;
+    } catch (const std::bad_alloc&) {
+        return set_error(NWB_ENOMEM, "nwb_pool_add: out of host memory");
+    }
+    if (A.geo != nwb::GEO_BOX)
+        return set_error(NWB_EINVAL, "nwb_pool_add: the pool takes axis-aligned affine (box) meshes");
+    for (int i = 0; i < nprobes; ++i)
+        if (probe_elem[i] < 0 || probe_elem[i] >= m->nelt)
+            return set_error(NWB_EINVAL, "nwb_pool_add: probe element out of range");
+    return admit(p, m->N, m->nelt, m->D, m->w3, A.egeo.data(), A.conn.data(), c0, dt, nsteps, nprobes,
+                 probe_elem, probe_w, energy_every, slot_out, nullptr);
+}
+
+nwb_status nwb_pool_add_box(nwb_pool* p, int N, int nelx, int nely, int nelz, double xmin,
+                            double xmax, double ymin, double ymax, double zmin, double zmax,
+                            int periodic_mask, double c0, double dt, int nsteps, int nprobes,
+                            const double* probe_xyz, int energy_every, int* slot_out) {
+    if (!p || !slot_out) return set_error(NWB_EINVAL, "nwb_pool_add_box: null argument");
+    const long long nelt = static_cast<long long>(nelx) * nely * nelz;
+    if (N < 2 || N > 10 || nelx < 1 || nely < 1 || nelz < 1 || nelt > (1 << 25) ||
+        nelt * N * N * N > 0x7fffffffLL || !(xmax > xmin) || !(ymax > ymin) || !(zmax > zmin) ||
+        nsteps < 1 || !std::isfinite(dt) || dt <= 0 || nprobes < 0 || nprobes > nwb::kMaxProbes ||
+        energy_every < 1 || (nprobes > 0 && !probe_xyz))
+        return set_error(NWB_EINVAL, "nwb_pool_add_box: bad arguments");
+    std::vector<double> z, w, D;
+    std::vector<nwb::ElemGeo> geo;
+    std::vector<int> conn, pe;
+    std::vector<double> pw;
+    const double lo[3] = {xmin, ymin, zmin}, hi[3] = {xmax, ymax, zmax};
+    try {
+        nwb::gll(N, z, w, D);
+        box_geometry(N, nelx, nely, nelz, lo, hi, periodic_mask, z, w, geo, conn);
+        box_probes(N, nelx, nely, nelz, lo, hi, z, nprobes, probe_xyz, pe, pw);
+    } catch (const std::bad_alloc&) {
+        return set_error(NWB_ENOMEM, "nwb_pool_add_box: out of host memory");
+    }
+    std::vector<double> w3(static_cast<size_t>(N) * N * N);
+    for (int k = 0; k < N; ++k)
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i) w3[i + N * (j + N * k)] = w[i] * w[j] * w[k];
+    SlotHost* h = nullptr;
+    nwb_status r = admit(p, N, static_cast<int>(nelt), D.data(), w3.data(), geo.data(), conn.data(), c0,
+                         dt, nsteps, nprobes, pe.data(), pw.data(), energy_every, slot_out, &h);
+    if (r != NWB_OK) return r;
+    h->is_box = true;
+    nwb::BoxPulse& b = h->box;
+    b = nwb::BoxPulse{};
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = lo[a];
+        b.h[a] = (hi[a] - lo[a]) / (a == 0 ? nelx : a == 1 ? nely : nelz);
+    }
+    b.nel[0] = nelx;
+    b.nel[1] = nely;
+    b.nel[2] = nelz;
+    b.N = N;
+    for (int i = 0; i < N; ++i) b.z[i] = z[i];
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_upload(nwb_pool* p, int s, const double* h, size_t n) {
+    if (!p || !h || s < 0 || s >= (p ? p->max_slots : 0))
+        return set_error(NWB_EINVAL, "nwb_pool_upload: bad argument");
+    SlotHost& sh = p->slots[s];
+    if (!sh.used) return set_error(NWB_ENOTFOUND, "nwb_pool_upload: slot %d is free", s);
+    if (n != 6 * static_cast<size_t>(sh.npts))
+        return set_error(NWB_EINVAL, "nwb_pool_upload: size %zu, expected 6*npts", n);
+    nwb_status r = p->rebuild_work();
+    if (r != NWB_OK) return r;
+    NWB_PCU(cudaMemcpy2DAsync(sh.dev.u[0], sizeof(double) * sh.stride, h, sizeof(double) * sh.npts,
+                              sizeof(double) * sh.npts, 6, cudaMemcpyHostToDevice, p->st));
+    NWB_PCU(cudaMemsetAsync(sh.dev.k, 0, sizeof(double) * 6 * sh.stride, p->st));
+    sh.dev.par = 0;
+    sh.dev.done = 0;
+    sh.dev.active = 0;
+    r = p->write_slot(s);
+    if (r != NWB_OK) return r;
+    // initial-state energy and probes (history index 0)
+    cudaError_t e = nwb::launch_batch_diag(p->d_slots, p->d_work, p->d_ntiles, 0, s, p->sms * 4, p->st);
+    if (e == cudaSuccess) e = nwb::launch_batch_epilogue(p->d_slots, p->max_slots, 0, s, p->d_counters, p->st);
+    if (e != cudaSuccess) return set_error(NWB_ECUDA, "nwb_pool_upload: %s", cudaGetErrorString(e));
+    p->launches += 2;
+    sh.dev.active = 1;
+    sh.uploaded = true;
+    return p->write_slot(s);
+}
+
+nwb_status nwb_pool_init_pulse(nwb_pool* p, int s, const double* pulse) {
+    if (!p || !pulse || s < 0 || s >= (p ? p->max_slots : 0))
+        return set_error(NWB_EINVAL, "nwb_pool_init_pulse: bad argument");
+    SlotHost& sh = p->slots[s];
+    if (!sh.used || !sh.is_box)
+        return set_error(NWB_ENOTFOUND, "nwb_pool_init_pulse: slot %d is not a box cavity", s);
+    nwb_status r = p->rebuild_work();
+    if (r != NWB_OK) return r;
+    nwb::BoxPulse b = sh.box;
+    for (int i = 0; i < 30; ++i) b.pulse[i] = pulse[i];
+    cudaError_t e = nwb::launch_box_pulse(b, sh.dev.u[0], sh.stride, p->st);
+    if (e != cudaSuccess) return set_error(NWB_ECUDA, "nwb_pool_init_pulse: %s", cudaGetErrorString(e));
+    NWB_PCU(cudaMemsetAsync(sh.dev.k, 0, sizeof(double) * 6 * sh.stride, p->st));
+    sh.dev.par = 0;
+    sh.dev.done = 0;
+    sh.dev.active = 0;
+    r = p->write_slot(s);
+    if (r != NWB_OK) return r;
+    e = nwb::launch_batch_diag(p->d_slots, p->d_work, p->d_ntiles, 0, s, p->sms * 4, p->st);
+    if (e == cudaSuccess) e = nwb::launch_batch_epilogue(p->d_slots, p->max_slots, 0, s, p->d_counters, p->st);
+    if (e != cudaSuccess) return set_error(NWB_ECUDA, "nwb_pool_init_pulse: %s", cudaGetErrorString(e));
+    p->launches += 3;
+    sh.dev.active = 1;
+    sh.uploaded = true;
+    return p->write_slot(s);
+}
+
+nwb_status nwb_pool_step(nwb_pool* p, int nsteps) {
+    if (!p || nsteps < 0) return set_error(NWB_EINVAL, "nwb_pool_step: bad argument");
+    nwb_status r = p->ensure_graph();
+    if (r != NWB_OK) return r;
+    for (int i = 0; i < nsteps; ++i) {
+        NWB_PCU(cudaGraphLaunch(p->graph, p->st));
+        p->launches += 7;
+    }
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_sync(nwb_pool* p) {
+    if (!p) return set_error(NWB_EINVAL, "nwb_pool_sync: null pool");
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_query(nwb_pool* p, int* status, int* done, int cap) {
+    if (!p || (!status && !done)) return set_error(NWB_EINVAL, "nwb_pool_query: bad argument");
+    std::vector<nwb::SlotDev> tmp(p->max_slots);
+    NWB_PCU(cudaMemcpyAsync(tmp.data(), p->d_slots, sizeof(nwb::SlotDev) * p->max_slots,
+                            cudaMemcpyDeviceToHost, p->st));
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    for (int s = 0; s < p->max_slots && s < cap; ++s) {
+        const SlotHost& h = p->slots[s];
+        int st = -1;
+        if (h.used) st = !h.uploaded ? 0 : (tmp[s].done >= tmp[s].nsteps ? 2 : 1);
+        if (h.used) {
+            p->slots[s].dev.done = tmp[s].done;
+            p->slots[s].dev.par = tmp[s].par;
+            p->slots[s].dev.active = tmp[s].active;
+        }
+        if (status) status[s] = st;
+        if (done) done[s] = h.used ? tmp[s].done : 0;
+    }
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_results(nwb_pool* p, int s, double* state, double* energy, double* probes) {
+    if (!p || s < 0 || s >= p->max_slots) return set_error(NWB_EINVAL, "nwb_pool_results: bad argument");
+    SlotHost& h = p->slots[s];
+    if (!h.used) return set_error(NWB_ENOTFOUND, "nwb_pool_results: slot %d is free", s);
+    nwb::SlotDev d;
+    NWB_PCU(cudaMemcpyAsync(&d, p->d_slots + s, sizeof(d), cudaMemcpyDeviceToHost, p->st));
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    if (state)
+        NWB_PCU(cudaMemcpy2DAsync(state, sizeof(double) * h.npts, d.u[d.par], sizeof(double) * h.stride,
+                                  sizeof(double) * h.npts, 6, cudaMemcpyDeviceToHost, p->st));
+    if (energy)
+        NWB_PCU(cudaMemcpyAsync(energy, d.energy, sizeof(double) * (h.nsteps + 1), cudaMemcpyDeviceToHost,
+                                p->st));
+    if (probes && h.nprobes)
+        NWB_PCU(cudaMemcpyAsync(probes, d.probes, sizeof(double) * 6 * h.nprobes * (h.nsteps + 1),
+                                cudaMemcpyDeviceToHost, p->st));
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_remove(nwb_pool* p, int s) {
+    if (!p || s < 0 || s >= p->max_slots) return set_error(NWB_EINVAL, "nwb_pool_remove: bad argument");
+    if (!p->slots[s].used) return set_error(NWB_ENOTFOUND, "nwb_pool_remove: slot %d is free", s);
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    p->release_slot(s);
+    nwb_status r = p->write_slot(s);  // zeroed descriptor: inactive, no buffers
+    p->work_dirty = true;
+    return r;
+}
+
+nwb_status nwb_pool_info(const nwb_pool* p, size_t* used_bytes, size_t* budget_bytes, int* slots_used,
+                         long long* launches) {
+    if (!p) return set_error(NWB_EINVAL, "nwb_pool_info: null pool");
+    if (used_bytes) *used_bytes = p->arena.used();
+    if (budget_bytes) *budget_bytes = p->arena.total();
+    if (slots_used) {
+        int n = 0;
+        for (const SlotHost& h : p->slots) n += h.used;
+        *slots_used = n;
+    }
+    if (launches) *launches = p->launches;
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_time_steps(nwb_pool* p, int nsteps, float* ms) {
+    if (!p || !ms || nsteps < 1) return set_error(NWB_EINVAL, "nwb_pool_time_steps: bad argument");
+    nwb_status r = p->ensure_graph();
+    if (r != NWB_OK) return r;
+    cudaEvent_t a, b;
+    NWB_PCU(cudaEventCreate(&a));
+    NWB_PCU(cudaEventCreate(&b));
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    NWB_PCU(cudaEventRecord(a, p->st));
+    r = nwb_pool_step(p, nsteps);
+    NWB_PCU(cudaEventRecord(b, p->st));
+    NWB_PCU(cudaEventSynchronize(b));
+    NWB_PCU(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return r;
+}
+
+nwb_status nwb_pool_destroy(nwb_pool* p) {
+    if (!p) return NWB_OK;
+    if (p->st) cudaStreamSynchronize(p->st);
+    p->drop_graph();
+    void* ptrs[] = {p->base, p->d_slots, p->d_work, p->d_ntiles, p->d_counters};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (p->st) cudaStreamDestroy(p->st);
+    delete p;
+    return NWB_OK;
+}
+
+}  // extern "C"

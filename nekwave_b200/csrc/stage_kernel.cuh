@@ -101,9 +101,12 @@ __device__ __forceinline__ void numerical_flux(T nx, T ny, T nz, T hc0, T dEx, T
     f[5] = -half * nxE_z - hc0 * nnH_z;
 }
 
-template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM, int MINB>
-__global__ void __launch_bounds__(EPB * KS * N * N, MINB)
-    stage_kernel(const StageParams P) {
+// One tile (EPB consecutive elements starting at e0) of one stage.  Called by
+// all threads of a block; threads tid >= EPB*KS*N*N take part in the barriers
+// only (the batched kernel runs every N in blocks of one fixed size).
+template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM>
+__device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
+                                           unsigned char* smem, const int tid) {
     using TC = typename std::conditional<F32, float, double>::type;
     constexpr int N2 = N * N, N3 = N2 * N;
     constexpr int TPE = KS * N2;          // threads per element
@@ -112,7 +115,6 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     constexpr int CS = EPB * N3;          // component stride in shared memory
     using L = SmemLayout<N, F32, EPB, KSMEM>;
 
-    extern __shared__ __align__(16) unsigned char smem[];
     double* s_u = reinterpret_cast<double*>(smem + L::u);
     double* s_k = reinterpret_cast<double*>(smem + L::k);
     double* s_D = reinterpret_cast<double*>(smem + L::D);
@@ -123,21 +125,20 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     if constexpr (F32) s_uc = reinterpret_cast<TC*>(smem + L::uc);
     else s_uc = reinterpret_cast<TC*>(s_u);
 
-    const int tid = threadIdx.x;
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
     const int loc = lt % N2;
     const int h = lt / N2;
     const int i = loc % N;
     const int j = loc / N;
-    const int e0 = blockIdx.x * EPB;
     const int nvalid = min(EPB, P.nelt - e0);
+    const bool loader = tid < NT;
     const int e = e0 + team;
     const bool active = team < nvalid;
     const long long S = P.stride;
 
     // ---- 1. stage u_in (+ D, geometry) then k in shared memory ---------------
-    {
+    if (loader) {
         const long long gbase = static_cast<long long>(e0) * N3;
         const int cnt = nvalid * N3;
 #pragma unroll
@@ -170,12 +171,12 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
                 asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a));
             }
         }
-        cp_async_commit();
     }
+    cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
     if constexpr (F32) {
-        const int cnt = nvalid * N3;
+        const int cnt = loader ? nvalid * N3 : 0;
 #pragma unroll
         for (int c = 0; c < 6; ++c)
             for (int x = tid; x < cnt; x += NT) s_uc[c * CS + x] = static_cast<float>(s_u[c * CS + x]);
@@ -265,7 +266,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     const double A = P.a, B = P.b, DT = P.dt;
     const long long ebase = static_cast<long long>(e) * N3;
 
-#pragma unroll
+#pragma unroll 1
     for (int kk = 0; kk < KPT; ++kk) {
         const int k = h * KPT + kk;
         if (KS > 1 && k >= N) break;
@@ -386,6 +387,13 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
             __stcs(P.u_out + c * S + g, s_u[c * CS + sl] + B * kn);
         }
     }
+}
+
+template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM, int MINB>
+__global__ void __launch_bounds__(EPB * KS * N * N, MINB)
+    stage_kernel(const StageParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    stage_tile<N, GEO, F32, KS, EPB, KSMEM>(P, blockIdx.x * EPB, smem, threadIdx.x);
 }
 
 // Launch of one variant.  The opt-in shared-memory size is set on the first
