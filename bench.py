@@ -51,6 +51,12 @@ def parse():
                    help="elements per axis; values other than 32 are for profiling only")
     p.add_argument("--variant", type=int, default=-1,
                    help="stage-kernel launch shape; -1 = autotune on the workload")
+    p.add_argument("--workload", choices=["c2", "batch", "serve"], default="c2",
+                   help="c2: periodic 32^3 N=8 (default, the headline); batch: 256 uneven PEC "
+                        "cavities in one pool; serve: Poisson request stream")
+    p.add_argument("--rates", type=str, default="0.5,1,2",
+                   help="serve: arrival rates as multiples of the measured serial service rate")
+    p.add_argument("--requests", type=int, default=24, help="serve: requests per rate")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up + timed steps (small case for ncu captures)")
     return p.parse_args()
@@ -221,6 +227,123 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_batch(args, rank, world):
+    """256 PEC cavities (uneven sizes, 4..9 points) advanced together in one pool:
+    one persistent launch per LSRK stage, one CUDA graph per step."""
+    import torch
+    from nekwave_b200 import DgSolver
+    from nekwave_b200.pool import CavityPool
+    from nekwave_b200.workloads import batch_instances
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    inst = batch_instances(256, seed=args.seed + rank, steps=args.steps)
+    budget = int(sum(3 * 6 * c.npts * 8 + c.nel[0] * c.nel[1] * c.nel[2] * 400 for c in inst) * 1.2
+                 + (1 << 30))
+    prec = args.precision
+    pool = CavityPool(budget, max_slots=len(inst), precision=prec)
+    slots = [pool.add_box(c.N, c.nel, c.lo, c.hi, c.c0, c.dt, c.nsteps, energy_every=50)
+             for c in inst]
+    for s, c in zip(slots, inst):
+        pool.init_pulse(s, c.pulses)
+    pool.step(args.warmup)
+    pool.sync()
+    for s, c in zip(slots, inst):          # back to t = 0 for the timed run
+        pool.init_pulse(s, c.pulses)
+    launches0 = pool.info()["launches"]
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        torch.cuda.synchronize()
+        ms = pool.time_steps(args.steps)
+        torch.cuda.synchronize()
+    launches = pool.info()["launches"] - launches0
+    total = sum(c.dof_stages for c in inst)
+    value = total / (ms / 1e3) / 1e9
+    finals = {s: pool.results(s, energy=False, probes=False)["state"] for s in slots[:32]}
+    pool.close()
+    # per-instance error of this precision against an FP64 pool (first 32 instances)
+    errs = []
+    if prec != "fp64":
+        ref = CavityPool(budget, max_slots=32, precision="fp64")
+        rs = [ref.add_box(c.N, c.nel, c.lo, c.hi, c.c0, c.dt, c.nsteps, energy_every=50)
+              for c in inst[:32]]
+        for s, c in zip(rs, inst[:32]):
+            ref.init_pulse(s, c.pulses)
+        ref.step(args.steps)
+        for s_ref, s in zip(rs, slots[:32]):
+            a = ref.results(s_ref, energy=False, probes=False)["state"]
+            errs.append(float(np.linalg.norm(finals[s] - a) / np.linalg.norm(a)))
+        ref.close()
+    # serial plain FP64 single-mesh path on the same instances (bounded sample)
+    ser_dof, ser_ms = 0, 0.0
+    for c in inst[:48]:
+        so = DgSolver("fp64")
+        so.initializeBox(c.N, c.nel, c.lo, c.hi, c.c0)
+        so.initPulse(c.pulses)
+        so.steps(c.dt, 3)
+        ser_ms += so.timeSteps(c.dt, c.nsteps, graph=True)
+        ser_dof += c.dof_stages
+        so.finalize()
+    serial = ser_dof / (ser_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_DOF_STAGE * total / 5 / args.steps / (ms / 1e3 / args.steps / 5) / 1e9
+    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == "fp64" else "f32-bulk/f64-lsrk", "data": "synthetic (seeded)",
+            "config": dict(workload="batch_256_pec_cavities", instances=len(inst),
+                           nodes=int(sum(c.npts for c in inst)), points_per_dir="4..9",
+                           elements_per_dir="2..12", steps_each=args.steps, precision=prec,
+                           l2="inputs larger than L2 (3 x %.2f GB)" % (total / 5 / args.steps / 6 * 8 / 1e9 / 1.0)),
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "batch_stage_kernel (+diag, epilogue)"},
+            "serial_fp64_single_mesh": {"value": serial, "unit": METRIC,
+                                        "sample": "first 48 instances solved one at a time with "
+                                                  "the single-mesh FP64 solver (CUDA graph per step)",
+                                        "speedup_batched": value / serial},
+            "error_vs_fp64": ({"rel_l2_max": max(errs), "rel_l2_median": float(np.median(errs)),
+                               "instances": len(errs)} if errs else None)}
+
+
+def run_serve(args, rank, world):
+    """Poisson stream of cavity solves served with continuous batching; p50/p99
+    latency and solves/s per arrival rate, next to the serial FP64 path."""
+    import torch
+    from nekwave_b200.serving import Server, latency_stats, serve_serial
+    from nekwave_b200.workloads import serving_requests
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.requests
+    # serial service rate from a short serial run (rate 1e9: back to back)
+    probe_reqs = serving_requests(max(4, n // 4), 1e9, seed=args.seed + 1000)
+    ser, ser_wall = serve_serial(probe_reqs, precision="fp64")
+    mu = len(probe_reqs) / ser_wall
+    rows = []
+    budget = int(float(os.environ.get("NWB_SERVE_BUDGET_GB", "100")) * (1 << 30))
+    for mult in [float(x) for x in args.rates.split(",")]:
+        reqs = serving_requests(n, mult * mu, seed=args.seed + int(mult * 100))
+        srv = Server(budget, max_slots=512, precision=args.precision)
+        res, wall = srv.run(reqs)
+        srv.close()
+        st = latency_stats(res)
+        rows.append(dict(rate_multiple=mult, rate_per_s=mult * mu, solves_per_s=n / wall,
+                         p50_s=st["p50"], p99_s=st["p99"], mean_s=st["mean"],
+                         gdof_stage_per_s=sum(r.dof_stages for r in reqs) / wall / 1e9))
+    serial_reqs = serving_requests(n, 1.0 * mu, seed=args.seed + 100)
+    sres, swall = serve_serial(serial_reqs, precision="fp64")
+    sst = latency_stats(sres)
+    best = max(rows, key=lambda r: r["solves_per_s"])
+    return {"metric": "solves/s", "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": world,
+            "steps": n, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
+            "data": "synthetic Poisson stream (seeded)",
+            "config": dict(workload="serving_poisson_pec_cavities", requests_per_rate=n,
+                           serial_service_rate_per_s=mu, max_elements_per_dir=48,
+                           points_per_dir="4..9", budget_gb=budget / (1 << 30)),
+            "serving": rows,
+            "serial_fp64": dict(rate_per_s=mu, solves_per_s=n / swall, p50_s=sst["p50"],
+                                p99_s=sst["p99"])}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -231,10 +354,16 @@ def main():
         if line is not None:
             print(json.dumps(line), flush=True)
         return
+    if args.workload in ("batch", "serve"):
+        fn = run_batch if args.workload == "batch" else run_serve
+        line = fn(args, rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
 
     import torch
     import torch.distributed as dist
-    from nekwave_b200 import DgSolver, Mesh
+    from nekwave_b200 import DgSolver
 
     torch.cuda.set_device(local)
     dist_on = world > 1
@@ -249,14 +378,17 @@ def main():
 
     N = WORKLOAD["N"]
     nel = (args.nel,) * 3
-    mesh = Mesh(N)
-    mesh.createBoxMesh(*nel, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, True, True, True)
-    npts = mesh.getTotalPoints()
-    dt = WORKLOAD["cfl"] * mesh.computeMinNodeDistance()
-    u0 = initial_state(mesh.getCoordX(), mesh.getCoordY(), mesh.getCoordZ(), args.seed + rank)
+    npts = nel[0] * nel[1] * nel[2] * N ** 3
+    from nekwave_b200.workloads import box_dxmin
+    dt = WORKLOAD["cfl"] * box_dxmin(N, nel, (0, 0, 0), (1, 1, 1))
+    r0 = np.random.Generator(np.random.PCG64(args.seed + rank)).uniform(0.3, 0.7, 3)
+    pulses = [(0.0, 0, 0, 0, 0.0)] * 2 + [(1.0, r0[0], r0[1], r0[2], WORKLOAD["sigma"])] + \
+        [(0.0, 0, 0, 0, 0.0)] * 3
     solver = DgSolver(args.precision)
-    solver.initialize(mesh, WORKLOAD["c0"])
-    solver.uploadState(u0)
+    solver.initializeBox(N, nel, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), WORKLOAD["c0"],
+                         periodic=(True, True, True))
+    solver.initPulse(pulses)
+    u0 = solver.downloadState()
     tune_ms = None
     if args.variant >= 0:
         solver.setVariant(args.variant)

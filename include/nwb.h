@@ -113,6 +113,18 @@ void nwb_box_mesh_destroy(nwb_box_mesh* m);
  * The solver runs on the current CUDA device, on its own stream. */
 nwb_status nwb_solver_create(const nwb_mesh_desc* mesh, double c0,
                              nwb_precision precision, nwb_solver** out);
+/* Solver on a box mesh built inside the library: the geometry of
+ * Mesh::createBoxMesh (src/mesh.cpp:683-843) computed per element from the box
+ * parameters, without per-node host arrays (large boxes need no host memory
+ * beyond the state).  periodic_mask as in nwb_box_mesh_create. */
+nwb_status nwb_solver_create_box(int N, int nelx, int nely, int nelz, double xmin, double xmax,
+                                 double ymin, double ymax, double zmin, double zmax,
+                                 int periodic_mask, double c0, nwb_precision precision,
+                                 nwb_solver** out);
+/* Device-generated initial state of a box solver: component c is
+ * pulse[5c] * exp(-|x - (pulse[5c+1..5c+3])|^2 / pulse[5c+4]^2), 0 where
+ * pulse[5c+4] <= 0. */
+nwb_status nwb_solver_init_pulse(nwb_solver* s, const double* pulse /* [30] */);
 /* n must be 6*npts (the reference asserts the same, src/dg_solver.cpp:244). */
 nwb_status nwb_upload_state(nwb_solver* s, const double* host_state, size_t n);
 nwb_status nwb_download_state(nwb_solver* s, double* host_state, size_t n);

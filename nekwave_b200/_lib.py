@@ -67,6 +67,9 @@ SIGNATURES = {
     "nwb_box_mesh_destroy": (None, [C.c_void_p]),
     "nwb_solver_create": (C.c_int, [C.POINTER(MeshDesc), C.c_double, C.c_int,
                                     C.POINTER(C.c_void_p)]),
+    "nwb_solver_create_box": (C.c_int, [C.c_int] * 4 + [C.c_double] * 6 +
+                              [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
+    "nwb_solver_init_pulse": (C.c_int, [C.c_void_p, _D]),
     "nwb_upload_state": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_download_state": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_step": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),

@@ -36,7 +36,7 @@ constexpr int bsmem() {
 template <int N, bool F32>
 __device__ __forceinline__ void run_tile(const StageParams& P, int e0, unsigned char* smem, int tid) {
     static_assert(BShape<N>::KS * BShape<N>::EPB * N * N <= kBatchThreads, "shape too large");
-    stage_tile<N, GEO_BOX, F32, BShape<N>::KS, BShape<N>::EPB, false>(P, e0, smem, tid);
+    stage_tile<N, GEO_BOX, F32, BShape<N>::KS, BShape<N>::EPB, false, false>(P, e0, smem, tid);
 }
 
 // Carpenter-Kennedy LSRK45 (src/dg_solver.cpp:58-69).

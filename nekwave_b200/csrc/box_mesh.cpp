@@ -10,7 +10,9 @@
 // neighbour (the match the reference finds by an O(N^4) coordinate search per
 // face, src/mesh.cpp:1049-1069).
 #include "nwb.h"
+#include "nwb_internal.h"
 
+#include <algorithm>
 #include <cmath>
 #include <new>
 #include <string>
@@ -134,6 +136,110 @@ void trilinear_point(const double c[8][3], double r, double s, double t, double*
     met[6] = invJ * (xs * yt - xt * ys);
     met[7] = invJ * (xt * yr - xr * yt);
     met[8] = invJ * (xr * ys - xs * yr);
+}
+
+// Per-element geometry of a box cavity, computed from the box parameters with
+// the reference's trilinear arithmetic at exactly the nodes the mesh analysis
+// samples (node 0 for J^{-T} and J, face point (0,0) for each face's normal and
+// lift), so it equals what nwb_box_mesh_create + analysis would produce.
+void box_geometry(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                  int pmask, const std::vector<double>& z, const std::vector<double>& w,
+                  std::vector<ElemGeo>& geo, std::vector<int>& conn) {
+    const int nelt = nelx * nely * nelz;
+    geo.assign(nelt, ElemGeo{});
+    conn.assign(6 * static_cast<size_t>(nelt), kConnPEC);
+    const double dx = (hi[0] - lo[0]) / nelx, dy = (hi[1] - lo[1]) / nely, dz = (hi[2] - lo[2]) / nelz;
+    const int last = N - 1;
+    // local (i,j,k) of face point (0,0) of faces 0..5 (src/mesh.cpp:959-976)
+    const int fi[6][3] = {{0, 0, 0}, {last, 0, 0}, {0, last, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, last}};
+    const double sgn[6] = {-1, 1, 1, -1, -1, 1};
+    const int row[6] = {1, 0, 1, 0, 2, 2};  // s, r, s, r, t, t
+    auto eidx = [=](int a, int b, int c) { return a + nelx * (b + nely * c); };
+    for (int ez = 0; ez < nelz; ++ez)
+        for (int ey = 0; ey < nely; ++ey)
+            for (int ex = 0; ex < nelx; ++ex) {
+                const double x0 = lo[0] + ex * dx, x1 = x0 + dx;
+                const double y0 = lo[1] + ey * dy, y1 = y0 + dy;
+                const double z0 = lo[2] + ez * dz, z1 = z0 + dz;
+                const double c[8][3] = {{x0, y0, z0}, {x1, y0, z0}, {x1, y1, z0}, {x0, y1, z0},
+                                        {x0, y0, z1}, {x1, y0, z1}, {x1, y1, z1}, {x0, y1, z1}};
+                const int e = eidx(ex, ey, ez);
+                ElemGeo& G = geo[e];
+                double J0;
+                trilinear_point(c, z[0], z[0], z[0], nullptr, &J0, G.met);
+                G.jdet = J0;
+                for (int f = 0; f < 6; ++f) {
+                    double J, met[9];
+                    trilinear_point(c, z[fi[f][0]], z[fi[f][1]], z[fi[f][2]], nullptr, &J, met);
+                    // row of J^{-T} for the face's reference direction: (r|s|t)_(x,y,z)
+                    const double Nx = sgn[f] * J * met[row[f] + 0];
+                    const double Ny = sgn[f] * J * met[row[f] + 3];
+                    const double Nz = sgn[f] * J * met[row[f] + 6];
+                    const double L = std::sqrt(Nx * Nx + Ny * Ny + Nz * Nz);
+                    G.nrm[f][0] = (L > 1e-14) ? (Nx / L) : 0.0;
+                    G.nrm[f][1] = (L > 1e-14) ? (Ny / L) : 0.0;
+                    G.nrm[f][2] = (L > 1e-14) ? (Nz / L) : 0.0;
+                    const double dA = L * (w[0] * w[0]);
+                    const double w3v = w[fi[f][0]] * w[fi[f][1]] * w[fi[f][2]];
+                    G.lift[f] = dA / (J * w3v);
+                }
+                int nb[6];
+                nb[0] = ey > 0 ? eidx(ex, ey - 1, ez) : ((pmask & 2) ? eidx(ex, nely - 1, ez) : -1);
+                nb[1] = ex < nelx - 1 ? eidx(ex + 1, ey, ez) : ((pmask & 1) ? eidx(0, ey, ez) : -1);
+                nb[2] = ey < nely - 1 ? eidx(ex, ey + 1, ez) : ((pmask & 2) ? eidx(ex, 0, ez) : -1);
+                nb[3] = ex > 0 ? eidx(ex - 1, ey, ez) : ((pmask & 1) ? eidx(nelx - 1, ey, ez) : -1);
+                nb[4] = ez > 0 ? eidx(ex, ey, ez - 1) : ((pmask & 4) ? eidx(ex, ey, nelz - 1) : -1);
+                nb[5] = ez < nelz - 1 ? eidx(ex, ey, ez + 1) : ((pmask & 4) ? eidx(ex, ey, 0) : -1);
+                const int opp[6] = {2, 3, 0, 1, 5, 4};
+                for (int f = 0; f < 6; ++f)
+                    conn[6 * static_cast<size_t>(e) + f] = nb[f] < 0 ? kConnPEC : ((nb[f] << 6) | (opp[f] << 3));
+            }
+}
+
+// ProbeManager::init (src/probe.cpp:33-96) on a box: first element whose box is
+// nearest, reference coordinates clamped to [-1,1], tensor Lagrange weights
+// (src/probe.cpp:11-30).
+void box_probes(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                const std::vector<double>& z, int nprobes, const double* xyz, std::vector<int>& elem,
+                std::vector<double>& wts) {
+    const double h[3] = {(hi[0] - lo[0]) / nelx, (hi[1] - lo[1]) / nely, (hi[2] - lo[2]) / nelz};
+    const int nel[3] = {nelx, nely, nelz};
+    elem.assign(nprobes, 0);
+    wts.assign(static_cast<size_t>(nprobes) * 3 * N, 0.0);
+    for (int q = 0; q < nprobes; ++q) {
+        // the nearest element per axis, lowest index on ties (argmin over e)
+        int best[3];
+        double ref[3];
+        for (int a = 0; a < 3; ++a) {
+            double bd = 1e300;
+            int bi = 0;
+            double br = 0;
+            for (int i = 0; i < nel[a]; ++i) {
+                const double x0 = lo[a] + i * h[a], x1 = x0 + h[a];
+                const double r = std::abs(x1 - x0) > 1e-14 ? 2.0 * (xyz[3 * q + a] - x0) / (x1 - x0) - 1.0 : 0.0;
+                const double d = std::max(0.0, std::max(-1.0 - r, r - 1.0));
+                if (d * d < bd) {
+                    bd = d * d;
+                    bi = i;
+                    br = std::max(-1.0, std::min(1.0, r));
+                }
+            }
+            best[a] = bi;
+            ref[a] = br;
+        }
+        elem[q] = best[0] + nelx * (best[1] + nely * best[2]);
+        for (int a = 0; a < 3; ++a) {
+            double* L = &wts[(static_cast<size_t>(q) * 3 + a) * N];
+            int hit = -1;
+            for (int i = 0; i < N; ++i)
+                if (std::abs(ref[a] - z[i]) < 1e-12) { hit = i; break; }
+            for (int i = 0; i < N; ++i) L[i] = hit >= 0 ? (i == hit ? 1.0 : 0.0) : 1.0;
+            if (hit >= 0) continue;
+            for (int i = 0; i < N; ++i)
+                for (int j = 0; j < N; ++j)
+                    if (i != j) L[i] *= (ref[a] - z[j]) / (z[i] - z[j]);
+        }
+    }
 }
 
 }  // namespace nwb

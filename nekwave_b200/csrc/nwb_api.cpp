@@ -11,6 +11,7 @@
 //     arrays (the general path).
 // One stage is one kernel launch; a time step is five launches, optionally
 // replayed from a CUDA graph.
+#include "batch.cuh"
 #include "nwb.h"
 #include "nwb_internal.h"
 
@@ -229,6 +230,8 @@ struct nwb_solver {
     size_t device_bytes = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     double gdt = 0.0;
+    bool is_box = false;
+    nwb::BoxPulse box{};
 
     nwb::StageParams params(int stage, double dt) const {
         nwb::StageParams P{};
@@ -340,6 +343,11 @@ struct nwb_solver {
     }
 };
 
+namespace {
+nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* D, const double* w3,
+                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out);
+}  // namespace
+
 extern "C" {
 
 const char* nwb_last_error(void) { return g_err.c_str(); }
@@ -391,7 +399,19 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
     } catch (const std::bad_alloc&) {
         return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");
     }
+    return create_solver(m, N, m->nelt, m->D, m->w3, A, c0, prec, out);
+}
 
+}  // extern "C"
+
+namespace {
+
+// Allocates and uploads a solver from analysed geometry.  m supplies the
+// per-node arrays of the general class and may be null for the affine classes.
+nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* D, const double* w3,
+                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out) {
+    const int N2 = N * N, N3 = N2 * N;
+    const long long npts = static_cast<long long>(nelt) * N3;
     nwb_solver* s = new (std::nothrow) nwb_solver();
     if (!s) return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");
     auto bail = [&](nwb_status r) {
@@ -405,14 +425,14 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
         return fail(NWB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(ce));
     }
     s->N = N;
-    s->nelt = m->nelt;
+    s->nelt = nelt;
     s->npts = npts;
     s->stride = (npts + 63) / 64 * 64;  // 512-byte aligned components
-    s->nfp = static_cast<long long>(m->nelt) * 6 * N2;
+    s->nfp = static_cast<long long>(nelt) * 6 * N2;
     s->geo = A.geo;
     s->f32 = prec == NWB_FP32_BULK ? 1 : 0;
     s->c0 = c0;
-    s->eblocks = nwb::energy_blocks(m->nelt);
+    s->eblocks = nwb::energy_blocks(nelt);
     ce = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce)));
 
@@ -437,15 +457,15 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
 #define NWB_H2D(dst, src, bytes) \
     do { ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
          if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
-    NWB_H2D(s->dD, m->D, sizeof(double) * N2);
-    NWB_H2D(s->dw3, m->w3, sizeof(double) * N3);
+    NWB_H2D(s->dD, D, sizeof(double) * N2);
+    NWB_H2D(s->dw3, w3, sizeof(double) * N3);
     if (s->geo != nwb::GEO_NODAL) {
-        NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(m->nelt), &tot));
-        NWB_TRY(dalloc(&s->dconn, 6 * static_cast<size_t>(m->nelt), &tot));
-        NWB_TRY(dalloc(&s->djac_e, static_cast<size_t>(m->nelt), &tot));
-        NWB_H2D(s->dgeo, A.egeo.data(), sizeof(nwb::ElemGeo) * m->nelt);
-        NWB_H2D(s->dconn, A.conn.data(), sizeof(int) * 6 * static_cast<size_t>(m->nelt));
-        NWB_H2D(s->djac_e, A.jac_e.data(), sizeof(double) * m->nelt);
+        NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(nelt), &tot));
+        NWB_TRY(dalloc(&s->dconn, 6 * static_cast<size_t>(nelt), &tot));
+        NWB_TRY(dalloc(&s->djac_e, static_cast<size_t>(nelt), &tot));
+        NWB_H2D(s->dgeo, A.egeo.data(), sizeof(nwb::ElemGeo) * nelt);
+        NWB_H2D(s->dconn, A.conn.data(), sizeof(int) * 6 * static_cast<size_t>(nelt));
+        NWB_H2D(s->djac_e, A.jac_e.data(), sizeof(double) * nelt);
     } else {
         const size_t nfp = static_cast<size_t>(s->nfp);
         try {
@@ -486,6 +506,68 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
 #undef NWB_TRY
 #undef NWB_H2D
     *out = s;
+    return NWB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nwb_status nwb_solver_create_box(int N, int nelx, int nely, int nelz, double xmin, double xmax,
+                                 double ymin, double ymax, double zmin, double zmax,
+                                 int periodic_mask, double c0, nwb_precision prec, nwb_solver** out) {
+    if (!out) return fail(NWB_EINVAL, "nwb_solver_create_box: out is null");
+    *out = nullptr;
+    const long long nelt = static_cast<long long>(nelx) * nely * nelz;
+    if (N < 2 || N > 10 || nelx < 1 || nely < 1 || nelz < 1 || nelt > (1 << 25) ||
+        nelt * N * N * N > 0x7fffffffLL || !(xmax > xmin) || !(ymax > ymin) || !(zmax > zmin))
+        return fail(NWB_EINVAL, "nwb_solver_create_box: bad box");
+    if (prec != NWB_FP64 && prec != NWB_FP32_BULK)
+        return fail(NWB_EINVAL, "nwb_solver_create_box: unknown precision %d", static_cast<int>(prec));
+    if (!std::isfinite(c0)) return fail(NWB_EINVAL, "nwb_solver_create_box: c0 not finite");
+    Analysis A;
+    std::vector<double> z, w, D, w3(static_cast<size_t>(N) * N * N);
+    const double lo[3] = {xmin, ymin, zmin}, hi[3] = {xmax, ymax, zmax};
+    try {
+        nwb::gll(N, z, w, D);
+        nwb::box_geometry(N, nelx, nely, nelz, lo, hi, periodic_mask, z, w, A.egeo, A.conn);
+    } catch (const std::bad_alloc&) {
+        return fail(NWB_ENOMEM, "nwb_solver_create_box: out of host memory");
+    }
+    for (int k = 0; k < N; ++k)
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i) w3[i + N * (j + N * k)] = w[i] * w[j] * w[k];
+    A.jac_e.resize(A.egeo.size());
+    bool box = true;
+    for (size_t e = 0; e < A.egeo.size(); ++e) {
+        A.jac_e[e] = A.egeo[e].jdet;
+        double scale = 0;
+        for (int c = 0; c < 9; ++c) scale = std::max(scale, std::abs(A.egeo[e].met[c]));
+        for (int c : {1, 2, 3, 5, 6, 7})
+            if (std::abs(A.egeo[e].met[c]) > 1e-13 * scale) box = false;
+    }
+    A.geo = box ? nwb::GEO_BOX : nwb::GEO_AFFINE;
+    nwb_status r = create_solver(nullptr, N, static_cast<int>(nelt), D.data(), w3.data(), A, c0, prec, out);
+    if (r != NWB_OK) return r;
+    nwb_solver* s = *out;
+    s->box.lo[0] = xmin; s->box.lo[1] = ymin; s->box.lo[2] = zmin;
+    s->box.h[0] = (xmax - xmin) / nelx; s->box.h[1] = (ymax - ymin) / nely; s->box.h[2] = (zmax - zmin) / nelz;
+    s->box.nel[0] = nelx; s->box.nel[1] = nely; s->box.nel[2] = nelz;
+    s->box.N = N;
+    for (int i = 0; i < N; ++i) s->box.z[i] = z[i];
+    s->is_box = true;
+    return NWB_OK;
+}
+
+nwb_status nwb_solver_init_pulse(nwb_solver* s, const double* pulse) {
+    if (!s || !pulse) return fail(NWB_EINVAL, "nwb_solver_init_pulse: null argument");
+    if (!s->is_box) return fail(NWB_EINVAL, "nwb_solver_init_pulse: solver was not created from a box");
+    nwb::BoxPulse b = s->box;
+    for (int i = 0; i < 30; ++i) b.pulse[i] = pulse[i];
+    cudaError_t e = nwb::launch_box_pulse(b, s->u[s->cur], s->stride, s->st);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "pulse kernel: %s", cudaGetErrorString(e));
+    ++s->launches;
+    NWB_CU(cudaStreamSynchronize(s->st));
     return NWB_OK;
 }
 

@@ -79,6 +79,17 @@ struct Analysis {
     std::vector<double> jac_e;
 };
 nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A);
+
+// Box meshes without per-node arrays (box_mesh.cpp).
+void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<double>& D);
+void trilinear_point(const double c[8][3], double r, double s, double t, double* X, double* J,
+                     double met[9]);
+void box_geometry(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                  int pmask, const std::vector<double>& z, const std::vector<double>& w,
+                  std::vector<ElemGeo>& geo, std::vector<int>& conn);
+void box_probes(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],
+                const std::vector<double>& z, int nprobes, const double* xyz, std::vector<int>& elem,
+                std::vector<double>& wts);
 nwb_status set_error(nwb_status s, const char* fmt, ...);
 
 // Fused stage kernel (stage_inst.cu, one object per N).  Variant 0 exists for

@@ -104,7 +104,7 @@ __device__ __forceinline__ void numerical_flux(T nx, T ny, T nz, T hc0, T dEx, T
 // One tile (EPB consecutive elements starting at e0) of one stage.  Called by
 // all threads of a block; threads tid >= EPB*KS*N*N take part in the barriers
 // only (the batched kernel runs every N in blocks of one fixed size).
-template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM>
+template <int N, int GEO, bool F32, int KS, int EPB, bool KSMEM, bool UNROLL_K = true>
 __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
                                            unsigned char* smem, const int tid) {
     using TC = typename std::conditional<F32, float, double>::type;
@@ -266,7 +266,9 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
     const double A = P.a, B = P.b, DT = P.dt;
     const long long ebase = static_cast<long long>(e) * N3;
 
-#pragma unroll 1
+    // the k-planes of a thread: unrolled (more independent work in flight) unless
+    // the caller must stay within a tight register budget
+#pragma unroll (UNROLL_K ? KPT : 1)
     for (int kk = 0; kk < KPT; ++kk) {
         const int k = h * KPT + kk;
         if (KS > 1 && k >= N) break;

@@ -47,6 +47,27 @@ class DgSolver:
         self._mesh = mesh
         return True
 
+    def initializeBox(self, N: int, nel, lo, hi, c0: float, periodic=(False, False, False)) -> bool:
+        """Box mesh built inside the library (geometry of Mesh::createBoxMesh per
+        element, no per-node host arrays), then as initialize()."""
+        self.finalize()
+        L = _lib.lib()
+        h = C.c_void_p()
+        mask = (1 if periodic[0] else 0) | (2 if periodic[1] else 0) | (4 if periodic[2] else 0)
+        check(L.nwb_solver_create_box(int(N), int(nel[0]), int(nel[1]), int(nel[2]), float(lo[0]),
+                                      float(hi[0]), float(lo[1]), float(hi[1]), float(lo[2]),
+                                      float(hi[2]), mask, float(c0), self._prec, C.byref(h)))
+        self._h = h
+        self._npts = int(nel[0]) * int(nel[1]) * int(nel[2]) * int(N) ** 3
+        self._mesh = None
+        return True
+
+    def initPulse(self, pulses) -> None:
+        """Device-generated Gaussian initial state (box solvers): pulses[c] =
+        (amp, x0, y0, z0, sigma) for component c of [Ex,Ey,Ez,Hx,Hy,Hz]."""
+        q = np.ascontiguousarray(np.asarray(pulses, dtype=np.float64).reshape(30))
+        check(_lib.lib().nwb_solver_init_pulse(self._need(), dptr(q)))
+
     def _need(self):
         if self._h is None:
             raise RuntimeError("DgSolver not initialized")

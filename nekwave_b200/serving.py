@@ -1,0 +1,129 @@
+"""Continuous-batching server of cavity solves on one GPU.
+
+Requests (box cavity, order, final time, Gaussian pulse, 8 probes) arrive on a
+stream.  The server admits them into a CavityPool in arrival order as HBM budget
+and slots free up, keeps their fields resident, advances every admitted cavity
+together (one persistent launch per LSRK stage for all of them), and as each
+finishes returns its probe traces and energy history and frees its memory.
+Requests that arrive while others are on the GPU join the running batch at the
+next step boundary.  Latency = completion time - arrival time.
+
+The serial baseline serves the same stream one request at a time with the
+single-mesh FP64 solver (DgSolver), the reference's execution model.
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass
+
+import numpy as np
+
+from .pool import FINISHED, CavityPool, PoolFull
+from .workloads import Cavity
+
+
+@dataclass
+class Result:
+    request: int
+    arrival: float
+    admitted: float
+    finished: float
+    probes: np.ndarray       # [nsteps+1, 8, 6]
+    energy: np.ndarray       # [nsteps+1] (NaN where not recorded)
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+class Server:
+    def __init__(self, hbm_budget_bytes: int, max_slots: int = 512, precision: str = "fp32",
+                 chunk: int = 4, energy_every: int = 10):
+        self.pool = CavityPool(hbm_budget_bytes, max_slots=max_slots, precision=precision)
+        self.chunk = int(chunk)
+        self.energy_every = int(energy_every)
+
+    def close(self):
+        self.pool.close()
+
+    def admit(self, req: Cavity):
+        s = self.pool.add_box(req.N, req.nel, req.lo, req.hi, req.c0, req.dt, req.nsteps,
+                              periodic=req.periodic, probes=req.probes,
+                              energy_every=self.energy_every)
+        self.pool.init_pulse(s, req.pulses)
+        return s
+
+    def run(self, requests, time_scale: float = 1.0, log=None):
+        """Serve the stream in real time (arrivals replayed at time_scale x the
+        request timestamps).  Returns the results in request order and the
+        wall time of the whole run."""
+        pending = deque()
+        arrivals = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
+        nxt = 0
+        running = {}            # slot -> (request index, admit time)
+        results = [None] * len(requests)
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        while nxt < len(arrivals) or pending or running:
+            t = now()
+            while nxt < len(arrivals) and requests[arrivals[nxt]].arrival * time_scale <= t:
+                pending.append(arrivals[nxt])
+                nxt += 1
+            while pending:                       # FIFO admission by HBM budget
+                i = pending[0]
+                try:
+                    s = self.admit(requests[i])
+                except PoolFull:
+                    break
+                pending.popleft()
+                running[s] = (i, now())
+            if not running:
+                if nxt < len(arrivals):          # idle until the next arrival
+                    wait = requests[arrivals[nxt]].arrival * time_scale - now()
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                continue
+            self.pool.step(self.chunk)
+            status, _ = self.pool.query()
+            for s in [s for s in running if status[s] == FINISHED]:
+                i, ta = running.pop(s)
+                r = self.pool.results(s, state=False)
+                results[i] = Result(i, requests[i].arrival * time_scale, ta, now(), r["probes"],
+                                    r["energy"])
+                self.pool.remove(s)
+                if log:
+                    log(results[i])
+        return results, now()
+
+
+def serve_serial(requests, precision="fp64", time_scale: float = 1.0):
+    """The same stream served one request at a time with the single-mesh solver,
+    the reference's execution model (box solver built per request, device initial
+    state, nsteps steps from a CUDA graph, final energy read back).  It records
+    no per-step probes or energy, which only favours it."""
+    from . import DgSolver
+    order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
+    results = [None] * len(requests)
+    t0 = time.perf_counter()
+    for i in order:
+        req = requests[i]
+        wait = req.arrival * time_scale - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        ta = time.perf_counter() - t0
+        s = DgSolver(precision)
+        s.initializeBox(req.N, req.nel, req.lo, req.hi, req.c0, periodic=req.periodic)
+        s.initPulse(req.pulses)
+        s.steps(req.dt, req.nsteps)
+        energy = np.array([s.energy()])
+        s.finalize()
+        results[i] = Result(i, req.arrival * time_scale, ta, time.perf_counter() - t0,
+                            np.zeros((0, 0, 6)), energy)
+    return results, time.perf_counter() - t0
+
+
+def latency_stats(results):
+    lat = np.array([r.latency for r in results if r is not None])
+    return dict(n=int(lat.size), p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
+                mean=float(lat.mean()), max=float(lat.max()))
