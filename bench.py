@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--rates", type=str, default="0.5,1,2",
                    help="serve: arrival rates as multiples of the measured serial service rate")
     p.add_argument("--requests", type=int, default=24, help="serve: requests per rate")
+    p.add_argument("--accuracy-steps", type=int, default=0,
+                   help="c2: also run FP64 and FP32-bulk this many steps from the same initial "
+                        "state and report the relative L2 error and energy drift")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up + timed steps (small case for ncu captures)")
     return p.parse_args()
@@ -291,7 +294,8 @@ def run_batch(args, rank, world):
             "config": dict(workload="batch_256_pec_cavities", instances=len(inst),
                            nodes=int(sum(c.npts for c in inst)), points_per_dir="4..9",
                            elements_per_dir="2..12", steps_each=args.steps, precision=prec,
-                           l2="inputs larger than L2 (3 x %.2f GB)" % (total / 5 / args.steps / 6 * 8 / 1e9 / 1.0)),
+                           l2="inputs larger than L2 (3 x %.2f GB)" % (
+                               sum(c.npts for c in inst) * 48 / 1e9)),
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
@@ -312,10 +316,13 @@ def run_serve(args, rank, world):
     from nekwave_b200.workloads import serving_requests
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     n = args.requests
-    # serial service rate from a short serial run (rate 1e9: back to back)
-    probe_reqs = serving_requests(max(4, n // 4), 1e9, seed=args.seed + 1000)
-    ser, ser_wall = serve_serial(probe_reqs, precision="fp64")
-    mu = len(probe_reqs) / ser_wall
+    # serial service rate: the serial path's GDOF-stage/s on a few requests over the
+    # mean work of a request of this distribution (2000 samples, no GPU work)
+    calib = serving_requests(4, 1e9, seed=args.seed + 1000)
+    _, cal_wall = serve_serial(calib, precision="fp64")
+    serial_rate = sum(c.dof_stages for c in calib) / cal_wall
+    mean_work = float(np.mean([c.dof_stages for c in serving_requests(2000, 1.0, seed=args.seed + 7)]))
+    mu = serial_rate / mean_work
     rows = []
     budget = int(float(os.environ.get("NWB_SERVE_BUDGET_GB", "100")) * (1 << 30))
     for mult in [float(x) for x in args.rates.split(",")]:
@@ -337,7 +344,8 @@ def run_serve(args, rank, world):
             "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
             "data": "synthetic Poisson stream (seeded)",
             "config": dict(workload="serving_poisson_pec_cavities", requests_per_rate=n,
-                           serial_service_rate_per_s=mu, max_elements_per_dir=48,
+                           serial_service_rate_per_s=mu, serial_gdof_stage_per_s=serial_rate / 1e9,
+                           mean_request_gdof_stage=mean_work / 1e9, max_elements_per_dir=48,
                            points_per_dir="4..9", budget_gb=budget / (1 << 30)),
             "serving": rows,
             "serial_fp64": dict(rate_per_s=mu, solves_per_s=n / swall, p50_s=sst["p50"],
@@ -453,6 +461,24 @@ def main():
     e2e_value = 6 * npts * 5 * e2e_steps * world / float(tt.item()) / 1e9
     del ctypes, ev0
 
+    accuracy = None
+    if args.accuracy_steps > 0:
+        out = {}
+        for prec in ("fp64", "fp32"):
+            a = DgSolver(prec)
+            a.initializeBox(N, nel, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), WORKLOAD["c0"],
+                            periodic=(True, True, True))
+            a.initPulse(pulses)
+            e0 = a.energy()
+            a.steps(dt, args.accuracy_steps)
+            out[prec] = (a.downloadState(), e0, a.energy())
+            a.finalize()
+        u64, u32 = out["fp64"][0], out["fp32"][0]
+        accuracy = {"steps": args.accuracy_steps,
+                    "fp32_rel_l2_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
+                    "energy_drift_fp64": (out["fp64"][2] - out["fp64"][1]) / out["fp64"][1],
+                    "energy_drift_fp32": (out["fp32"][2] - out["fp32"][1]) / out["fp32"][1]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate()
@@ -489,6 +515,8 @@ def main():
                     "steps": e2e_steps,
                     "pattern": "uploadState (pinned) + step + downloadState per step"},
         }
+        if accuracy is not None:
+            line["accuracy"] = accuracy
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

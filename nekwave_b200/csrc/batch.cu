@@ -16,17 +16,18 @@ namespace {
 using stage::SmemLayout;
 using stage::stage_tile;
 
-// Shape per N for 256-thread blocks: KS threads per column, EPB elements.
+// Shape per N for the batch kernel's blocks (kBatchThreads = 128): KS threads
+// per column, EPB elements -- the single-mesh kernel's fastest shapes that fit.
 template <int N> struct BShape;
-template <> struct BShape<2> { static constexpr int KS = 2, EPB = 32; };
-template <> struct BShape<3> { static constexpr int KS = 3, EPB = 9; };
-template <> struct BShape<4> { static constexpr int KS = 4, EPB = 4; };
-template <> struct BShape<5> { static constexpr int KS = 5, EPB = 2; };
-template <> struct BShape<6> { static constexpr int KS = 6, EPB = 1; };
-template <> struct BShape<7> { static constexpr int KS = 5, EPB = 1; };
-template <> struct BShape<8> { static constexpr int KS = 4, EPB = 1; };
-template <> struct BShape<9> { static constexpr int KS = 3, EPB = 1; };
-template <> struct BShape<10> { static constexpr int KS = 2, EPB = 1; };
+template <> struct BShape<2> { static constexpr int KS = 2, EPB = 16; };
+template <> struct BShape<3> { static constexpr int KS = 1, EPB = 14; };
+template <> struct BShape<4> { static constexpr int KS = 1, EPB = 8; };
+template <> struct BShape<5> { static constexpr int KS = 1, EPB = 4; };
+template <> struct BShape<6> { static constexpr int KS = 3, EPB = 1; };
+template <> struct BShape<7> { static constexpr int KS = 1, EPB = 2; };
+template <> struct BShape<8> { static constexpr int KS = 2, EPB = 1; };
+template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1; };
+template <> struct BShape<10> { static constexpr int KS = 1, EPB = 1; };
 
 template <int N, bool F32>
 constexpr int bsmem() {
@@ -51,7 +52,7 @@ __constant__ double c_rk4b[5] = {1432997174477.0 / 9575080441755.0,
                                  2277821191437.0 / 14882151754819.0};
 
 template <bool F32>
-__global__ void __launch_bounds__(kBatchThreads, 2)
+__global__ void __launch_bounds__(kBatchThreads, 4)
 batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
                    const int* __restrict__ ntiles_p, int* __restrict__ counters, int stage) {
     extern __shared__ __align__(16) unsigned char smem[];

@@ -5,7 +5,7 @@
 
 namespace nwb {
 
-constexpr int kBatchThreads = 256;  // block size of the persistent batch kernel
+constexpr int kBatchThreads = 128;  // block size of the persistent batch kernel
 constexpr int kMaxProbes = 8;
 
 // One resident cavity ("slot") as the device sees it.  All pointers are

@@ -202,7 +202,7 @@ struct nwb_pool {
         NWB_PCU(nwb::batch_prepare(f32, graph_smem));
         // persistent grid: as many resident blocks as the shared memory allows
         const int by_smem = std::max(1, (227 * 1024) / (graph_smem + 1024));
-        grid = sms * std::min(2, by_smem);
+        grid = sms * std::min(4, by_smem);
         diag_grid = sms * 4;
         cudaGraph_t g = nullptr;
         NWB_PCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));

@@ -176,23 +176,32 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
     cp_async_wait<1>();
     __syncthreads();
     if constexpr (F32) {
+        // FP32 copy of the tile as deviations from the element's centre node:
+        // the derivatives are unchanged (rows of D sum to zero) and the rounding
+        // error scales with the variation across the element instead of |u|
+        constexpr int centre = (N / 2) * (1 + N + N2);
         const int cnt = loader ? nvalid * N3 : 0;
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-            for (int x = tid; x < cnt; x += NT) s_uc[c * CS + x] = static_cast<float>(s_u[c * CS + x]);
+            for (int x = tid; x < cnt; x += NT) {
+                const double ref = s_u[c * CS + (x / N3) * N3 + centre];
+                s_uc[c * CS + x] = static_cast<float>(s_u[c * CS + x] - ref);
+            }
         __syncthreads();
     }
 
     // ---- 2. face phase: lifted numerical flux per face point -----------------
     if (active) {
-        const TC* U = s_uc + team * N3;
+        // traces and jumps in FP64 in both precision classes: a jump is a small
+        // difference of two nearly equal traces and is rounded only afterwards
+        const double* U = s_u + team * N3;
         for (int fp = lt; fp < 6 * N2; fp += TPE) {
             const int f = fp / N2;
             const int pq = fp - f * N2;
             const int p = pq % N, q = pq / N;
             const int m = face_local<N>(f, p, q);
-            const TC Exm = U[0 * CS + m], Eym = U[1 * CS + m], Ezm = U[2 * CS + m];
-            const TC Hxm = U[3 * CS + m], Hym = U[4 * CS + m], Hzm = U[5 * CS + m];
+            const double Exm = U[0 * CS + m], Eym = U[1 * CS + m], Ezm = U[2 * CS + m];
+            const double Hxm = U[3 * CS + m], Hym = U[4 * CS + m], Hzm = U[5 * CS + m];
             long long vB = -1;  // neighbour node (global index), -1 = mirror
             double nxd, nyd, nzd, lift;
             if constexpr (GEO == GEO_NODAL) {
@@ -218,28 +227,31 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
                 nzd = G.nrm[f][2];
                 lift = G.lift[f];
             }
-            TC dEx, dEy, dEz, dHx, dHy, dHz;
+            double jmp[6];
             if (vB < 0) {
                 // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
-                dEx = TC(-2) * Exm; dEy = TC(-2) * Eym; dEz = TC(-2) * Ezm;
-                dHx = TC(0); dHy = TC(0); dHz = TC(0);
+                jmp[0] = -2.0 * Exm; jmp[1] = -2.0 * Eym; jmp[2] = -2.0 * Ezm;
+                jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
             } else {
                 const long long eB = vB / N3;
-                TC vals[6];
+                double vals[6];
                 if (eB >= e0 && eB < e0 + nvalid) {
                     const int sidx = static_cast<int>(vB - static_cast<long long>(e0) * N3);
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) vals[c] = s_uc[c * CS + sidx];
+                    for (int c = 0; c < 6; ++c) vals[c] = s_u[c * CS + sidx];
                 } else {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) vals[c] = static_cast<TC>(__ldg(P.u_in + c * S + vB));
+                    for (int c = 0; c < 6; ++c) vals[c] = __ldg(P.u_in + c * S + vB);
                 }
-                dEx = vals[0] - Exm; dEy = vals[1] - Eym; dEz = vals[2] - Ezm;
-                dHx = vals[3] - Hxm; dHy = vals[4] - Hym; dHz = vals[5] - Hzm;
+                jmp[0] = vals[0] - Exm; jmp[1] = vals[1] - Eym; jmp[2] = vals[2] - Ezm;
+                jmp[3] = vals[3] - Hxm; jmp[4] = vals[4] - Hym; jmp[5] = vals[5] - Hzm;
             }
             TC fl[6];
             numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
-                               static_cast<TC>(0.5 * P.c0), dEx, dEy, dEz, dHx, dHy, dHz, fl);
+                               static_cast<TC>(0.5 * P.c0), static_cast<TC>(jmp[0]),
+                               static_cast<TC>(jmp[1]), static_cast<TC>(jmp[2]),
+                               static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
+                               static_cast<TC>(jmp[5]), fl);
             double* F = s_flux + (team * 6 + f) * 6 * N2 + pq;
 #pragma unroll
             for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
