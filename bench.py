@@ -247,6 +247,7 @@ def run_batch(args, rank, world):
              for c in inst]
     for s, c in zip(slots, inst):
         pool.init_pulse(s, c.pulses)
+    mode, mode_ms = pool.autotune(reps=5)
     pool.step(args.warmup)
     pool.sync()
     for s, c in zip(slots, inst):          # back to t = 0 for the timed run
@@ -292,6 +293,8 @@ def run_batch(args, rank, world):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == "fp64" else "f32-bulk/f64-lsrk", "data": "synthetic (seeded)",
             "config": dict(workload="batch_256_pec_cavities", instances=len(inst),
+                           launch_mode=("one launch per N" if mode else "one persistent launch"),
+                           autotune_stage_ms=mode_ms,
                            nodes=int(sum(c.npts for c in inst)), points_per_dir="4..9",
                            elements_per_dir="2..12", steps_each=args.steps, precision=prec,
                            l2="inputs larger than L2 (3 x %.2f GB)" % (

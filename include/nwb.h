@@ -242,6 +242,14 @@ nwb_status nwb_pool_results(nwb_pool* p, int slot, double* state, double* energy
 nwb_status nwb_pool_remove(nwb_pool* p, int slot);
 nwb_status nwb_pool_info(const nwb_pool* p, size_t* used_bytes, size_t* budget_bytes,
                          int* slots_used, long long* launches);
+/* Stage launch mode: 0 = one persistent launch per stage for every N (tiles
+ * handed out by an atomic counter, largest first), 1 = one launch per N present,
+ * each with that N's tuned single-mesh launch shape, as parallel branches of the
+ * step graph.  nwb_pool_autotune times both on the resident cavities (timing
+ * launches with a = b = dt = 0 leave every state as it is) and keeps the faster;
+ * ms_out (optional) receives the two per-step stage times. */
+nwb_status nwb_pool_set_mode(nwb_pool* p, int mode);
+nwb_status nwb_pool_autotune(nwb_pool* p, int reps, int* best_mode, float* ms_out);
 /* Device time (ms, CUDA events on the pool's stream) of nsteps pool steps. */
 nwb_status nwb_pool_time_steps(nwb_pool* p, int nsteps, float* ms);
 nwb_status nwb_pool_destroy(nwb_pool* p);

@@ -101,6 +101,8 @@ SIGNATURES = {
     "nwb_pool_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                 _I, C.POINTER(C.c_longlong)]),
     "nwb_pool_time_steps": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    "nwb_pool_set_mode": (C.c_int, [C.c_void_p, C.c_int]),
+    "nwb_pool_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "nwb_pool_destroy": (C.c_int, [C.c_void_p]),
     "nwb_time_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int,
                                  C.POINTER(C.c_float)]),

@@ -54,7 +54,7 @@ __constant__ double c_rk4b[5] = {1432997174477.0 / 9575080441755.0,
 template <bool F32>
 __global__ void __launch_bounds__(kBatchThreads, 4)
 batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
-                   const int* __restrict__ ntiles_p, int* __restrict__ counters, int stage) {
+                   const int* __restrict__ ntiles_p, int* __restrict__ counters, int stage, int dry) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_tile;
     const int tid = threadIdx.x;
@@ -85,9 +85,9 @@ batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict
         P.fplus = nullptr;
         P.nfp = 0;
         P.c0 = S.c0;
-        P.a = c_rk4a[stage];
-        P.b = c_rk4b[stage];
-        P.dt = S.dt;
+        P.a = dry ? 0.0 : c_rk4a[stage];
+        P.b = dry ? 0.0 : c_rk4b[stage];
+        P.dt = dry ? 0.0 : S.dt;
         switch (w.N) {
             case 2: run_tile<2, F32>(P, w.e0, smem, tid); break;
             case 3: run_tile<3, F32>(P, w.e0, smem, tid); break;
@@ -101,6 +101,76 @@ batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict
             default: break;
         }
     }
+}
+
+// Stage parameters of one tile's slot.
+__device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, int dry) {
+    const int par = S.par ^ (stage & 1);
+    StageParams P;
+    P.u_in = S.u[par];
+    P.u_out = S.u[par ^ 1];
+    P.k = S.k;
+    P.stride = S.stride;
+    P.nelt = S.nelt;
+    P._pad0 = 0;
+    P.D = S.D;
+    P.geo = S.geo;
+    P.conn = S.conn;
+    P.met_n = nullptr;
+    P.fnrm = nullptr;
+    P.flift = nullptr;
+    P.fplus = nullptr;
+    P.nfp = 0;
+    P.c0 = S.c0;
+    P.a = dry ? 0.0 : c_rk4a[stage];
+    P.b = dry ? 0.0 : c_rk4b[stage];
+    P.dt = dry ? 0.0 : S.dt;
+    return P;
+}
+
+// One block per tile of one N: the single-mesh kernel's tuned shape for that N,
+// fully unrolled, reading its slot from the work item (per-N mode).
+template <int N, bool F32, int KS, int EPB, bool KSMEM, int MINB>
+__global__ void __launch_bounds__(EPB * KS * N * N, MINB)
+batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
+                     int stage, int dry) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WorkItem w = work[blockIdx.x];
+    const SlotDev& S = slots[w.slot];
+    if (!S.active) return;
+    const StageParams P = slot_params(S, stage, dry);
+    stage_tile<N, GEO_BOX, F32, KS, EPB, KSMEM, true>(P, w.e0, smem, threadIdx.x);
+}
+
+// Per-N shapes of the per-N mode: the single-mesh defaults (stage_variants.h entry 0).
+template <int N> struct NShape;
+template <> struct NShape<2> { static constexpr int KS = 2, EPB = 16, KSM = 1, MINB = 1; };
+template <> struct NShape<3> { static constexpr int KS = 1, EPB = 16, KSM = 0, MINB = 4; };
+template <> struct NShape<4> { static constexpr int KS = 1, EPB = 8, KSM = 0, MINB = 4; };
+template <> struct NShape<5> { static constexpr int KS = 1, EPB = 4, KSM = 0, MINB = 4; };
+template <> struct NShape<6> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 3; };
+template <> struct NShape<7> { static constexpr int KS = 1, EPB = 2, KSM = 0, MINB = 3; };
+template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4; };
+template <> struct NShape<9> { static constexpr int KS = 3, EPB = 1, KSM = 0, MINB = 2; };
+template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2; };
+
+template <int N, bool F32>
+cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
+                     cudaStream_t st, int* epb_out) {
+    using Sh = NShape<N>;
+    constexpr int threads = Sh::EPB * Sh::KS * N * N;
+    constexpr int smem = SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total;
+    auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB>;
+    if (epb_out) *epb_out = Sh::EPB;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (ntiles <= 0) return cudaSuccess;
+    kern<<<ntiles, threads, smem, st>>>(slots, work, stage, dry);
+    return cudaGetLastError();
 }
 
 // Does this slot record energy after the step it is taking now (post = 1), or
@@ -240,6 +310,28 @@ int max_batch_smem() {
 
 }  // namespace
 
+cudaError_t launch_batch_stage_n(int N, int f32, int stage, const SlotDev* slots,
+                                 const WorkItem* work, int ntiles, int dry, cudaStream_t st) {
+    switch (N) {
+#define NWB_CASE(n) \
+        case n: return f32 ? launch_n<n, true>(stage, slots, work, ntiles, dry, st, nullptr) \
+                           : launch_n<n, false>(stage, slots, work, ntiles, dry, st, nullptr);
+        NWB_CASE(2) NWB_CASE(3) NWB_CASE(4) NWB_CASE(5) NWB_CASE(6) NWB_CASE(7) NWB_CASE(8)
+        NWB_CASE(9) NWB_CASE(10)
+#undef NWB_CASE
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int batch_epb_n(int N) {
+    switch (N) {
+        case 2: return NShape<2>::EPB; case 3: return NShape<3>::EPB; case 4: return NShape<4>::EPB;
+        case 5: return NShape<5>::EPB; case 6: return NShape<6>::EPB; case 7: return NShape<7>::EPB;
+        case 8: return NShape<8>::EPB; case 9: return NShape<9>::EPB; case 10: return NShape<10>::EPB;
+        default: return 1;
+    }
+}
+
 BatchShape batch_shape(int N, int f32) {
     (void)f32;
     switch (N) {
@@ -281,12 +373,12 @@ cudaError_t batch_prepare(int f32, int smem) {
 }
 
 cudaError_t launch_batch_stage(int f32, int stage, const SlotDev* slots, const WorkItem* work,
-                               const int* ntiles, int* counters, int grid, int smem,
+                               const int* ntiles, int* counters, int grid, int smem, int dry,
                                cudaStream_t st) {
     if (f32)
-        batch_stage_kernel<true><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage);
+        batch_stage_kernel<true><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage, dry);
     else
-        batch_stage_kernel<false><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage);
+        batch_stage_kernel<false><<<grid, kBatchThreads, smem, st>>>(slots, work, ntiles, counters, stage, dry);
     return cudaGetLastError();
 }
 

@@ -48,9 +48,15 @@ struct BatchShape {
 
 // Batch launchers (batch.cu).
 // stage: 0..4.  counters[stage] is the dynamic tile counter of that stage.
+// dry = 1 runs the stage with a = b = dt = 0 (timing only: u_out = u_in, k = 0).
 cudaError_t launch_batch_stage(int f32, int stage, const SlotDev* slots, const WorkItem* work,
-                               const int* ntiles, int* counters, int grid, int smem,
+                               const int* ntiles, int* counters, int grid, int smem, int dry,
                                cudaStream_t st);
+// Per-N mode: one block per tile of the given N (work points at that N's tiles,
+// which must have been cut with batch_epb_n(N) elements each).
+cudaError_t launch_batch_stage_n(int N, int f32, int stage, const SlotDev* slots,
+                                 const WorkItem* work, int ntiles, int dry, cudaStream_t st);
+int batch_epb_n(int N);
 // Diagnostics after a step (post = 1) or of the initial state (post = 0):
 // energy partials per tile and probe values into the slots' history buffers.
 // only_slot >= 0 restricts the work to one slot (initial-state diagnostics).

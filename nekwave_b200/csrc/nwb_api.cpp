@@ -659,7 +659,7 @@ nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info) {
     info->ksmem = s->cfg.ksmem;
     info->minb = s->cfg.minb;
     info->variant = s->variant;
-    info->variant_count = nwb::stage_variant_count(s->N, s->geo);
+    info->variant_count = nwb::stage_variant_count(s->N, s->geo, s->f32);
     info->device_bytes = static_cast<long long>(s->device_bytes);
     return NWB_OK;
 }
@@ -679,7 +679,7 @@ nwb_status nwb_solver_launch_count(const nwb_solver* s, long long* count) {
 
 nwb_status nwb_solver_set_variant(nwb_solver* s, int variant) {
     if (!s) return fail(NWB_EINVAL, "nwb_solver_set_variant: null solver");
-    if (variant < 0 || variant >= nwb::stage_variant_count(s->N, s->geo))
+    if (variant < 0 || variant >= nwb::stage_variant_count(s->N, s->geo, s->f32))
         return fail(NWB_EINVAL, "nwb_solver_set_variant: variant %d out of range", variant);
     nwb::StageConfig c{};
     cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, variant, nullptr, nullptr, &c);
@@ -697,7 +697,7 @@ nwb_status nwb_solver_set_variant(nwb_solver* s, int variant) {
 // stage of every step multiplies by a = 0 anyway).
 nwb_status nwb_solver_autotune(nwb_solver* s, int reps, int* best, float* ms_out, int ms_cap) {
     if (!s || reps < 1) return fail(NWB_EINVAL, "nwb_solver_autotune: bad argument");
-    const int nv = nwb::stage_variant_count(s->N, s->geo);
+    const int nv = nwb::stage_variant_count(s->N, s->geo, s->f32);
     cudaEvent_t a, b;
     NWB_CU(cudaEventCreate(&a));
     NWB_CU(cudaEventCreate(&b));

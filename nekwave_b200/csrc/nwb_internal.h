@@ -99,12 +99,12 @@ nwb_status set_error(nwb_status s, const char* fmt, ...);
 // one-time kernel attribute set-up).
 cudaError_t launch_stage(int N, int geo, int f32, int variant, const StageParams* p,
                          cudaStream_t st, StageConfig* cfg_out);
-int stage_variant_count(int N, int geo);
+int stage_variant_count(int N, int geo, int f32);
 template <int N>
 cudaError_t launch_stage_n(int geo, int f32, int variant, const StageParams* p, cudaStream_t st,
                            StageConfig* cfg);
 template <int N>
-int stage_variant_count_n(int geo);
+int stage_variant_count_n(int geo, int f32);
 
 // FP64 energy of the state u (diag_kernels.cu): nblocks partial sums, then one
 // fixed-order final sum into *out (device).  J comes from jac_e (per element,

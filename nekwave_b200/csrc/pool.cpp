@@ -119,6 +119,13 @@ struct nwb_pool {
     bool work_dirty = true;
     int ntiles = 0;
     int smem_needed = 0;
+    // per-N mode: tiles cut with each N's own elements-per-block, grouped by N
+    nwb::WorkItem* d_work_n = nullptr;
+    int work_n_cap = 0;
+    int n_off[11] = {}, n_cnt[11] = {};
+    int mode = 0;  // 0: one persistent launch for every N, 1: one launch per N
+    cudaStream_t side[11] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[11] = {};
     cudaGraphExec_t graph = nullptr;
     int graph_smem = -1;
     int grid = 0, diag_grid = 0;
@@ -163,6 +170,27 @@ struct nwb_pool {
             return ca > cb;
         });
         ntiles = static_cast<int>(w.size());
+        std::vector<nwb::WorkItem> wn;
+        for (int N = 2; N <= 10; ++N) {
+            n_off[N] = static_cast<int>(wn.size());
+            const int epb = nwb::batch_epb_n(N);
+            for (int s = 0; s < max_slots; ++s) {
+                const SlotHost& h = slots[s];
+                if (!h.used || h.N != N) continue;
+                for (int e0 = 0; e0 < h.nelt; e0 += epb) wn.push_back(nwb::WorkItem{s, e0, N, 0});
+            }
+            n_cnt[N] = static_cast<int>(wn.size()) - n_off[N];
+        }
+        if (static_cast<int>(wn.size()) > work_n_cap) {
+            if (d_work_n) cudaFree(d_work_n);
+            d_work_n = nullptr;
+            work_n_cap = std::max(static_cast<int>(wn.size()), 2 * work_n_cap);
+            NWB_PCU(cudaMalloc(&d_work_n, sizeof(nwb::WorkItem) * work_n_cap));
+        }
+        if (!wn.empty())
+            NWB_PCU(cudaMemcpyAsync(d_work_n, wn.data(), sizeof(nwb::WorkItem) * wn.size(),
+                                    cudaMemcpyHostToDevice, st));
+        if (mode == 1) drop_graph();  // per-N grids follow the tile counts
         if (ntiles > work_cap) {
             if (d_work) cudaFree(d_work);
             d_work = nullptr;
@@ -179,16 +207,55 @@ struct nwb_pool {
         return NWB_OK;
     }
 
-    nwb_status launch_step() {
+    nwb_status launch_stages(int dry) {
         for (int s = 0; s < 5; ++s) {
-            cudaError_t e = nwb::launch_batch_stage(f32, s, d_slots, d_work, d_ntiles, d_counters,
-                                                    grid, graph_smem, st);
-            if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch stage: %s", cudaGetErrorString(e));
+            if (mode == 0) {
+                cudaError_t e = nwb::launch_batch_stage(f32, s, d_slots, d_work, d_ntiles, d_counters,
+                                                        grid, graph_smem, dry, st);
+                if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch stage: %s", cudaGetErrorString(e));
+                continue;
+            }
+            // one launch per N on its own stream: independent branches of the graph
+            NWB_PCU(cudaEventRecord(fork_ev, st));
+            for (int N = 2; N <= 10; ++N) {
+                if (!n_cnt[N]) continue;
+                NWB_PCU(cudaStreamWaitEvent(side[N], fork_ev, 0));
+                cudaError_t e = nwb::launch_batch_stage_n(N, f32, s, d_slots, d_work_n + n_off[N], n_cnt[N],
+                                                          dry, side[N]);
+                if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch stage N=%d: %s", N, cudaGetErrorString(e));
+                NWB_PCU(cudaEventRecord(join_ev[N], side[N]));
+                NWB_PCU(cudaStreamWaitEvent(st, join_ev[N], 0));
+            }
         }
+        return NWB_OK;
+    }
+
+    nwb_status launch_step() {
+        nwb_status r = launch_stages(0);
+        if (r != NWB_OK) return r;
         cudaError_t e = nwb::launch_batch_diag(d_slots, d_work, d_ntiles, 1, -1, diag_grid, st);
         if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch diag: %s", cudaGetErrorString(e));
         e = nwb::launch_batch_epilogue(d_slots, max_slots, 1, -1, d_counters, st);
         if (e != cudaSuccess) return set_error(NWB_ECUDA, "batch epilogue: %s", cudaGetErrorString(e));
+        return NWB_OK;
+    }
+
+    // Captures the five stages (dry = 1: timing only) or a whole step (dry = 0).
+    nwb_status capture(int dry, cudaGraphExec_t* out) {
+        cudaGraph_t g = nullptr;
+        NWB_PCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        // a timing graph has no epilogue to reset the tile counters: reset them first
+        if (dry) NWB_PCU(cudaMemsetAsync(d_counters, 0, sizeof(int) * 8, st));
+        nwb_status r = dry ? launch_stages(1) : launch_step();
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (r != NWB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(out, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "instantiate: %s", cudaGetErrorString(ce));
         return NWB_OK;
     }
 
@@ -204,19 +271,11 @@ struct nwb_pool {
         const int by_smem = std::max(1, (227 * 1024) / (graph_smem + 1024));
         grid = sms * std::min(4, by_smem);
         diag_grid = sms * 4;
-        cudaGraph_t g = nullptr;
-        NWB_PCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        r = launch_step();
-        cudaError_t ce = cudaStreamEndCapture(st, &g);
-        if (r != NWB_OK) {
-            if (g) cudaGraphDestroy(g);
-            return r;
+        for (int N = 2; N <= 10; ++N) {  // one-time kernel attribute set-up, outside capture
+            cudaError_t e = nwb::launch_batch_stage_n(N, f32, 0, nullptr, nullptr, 0, 0, st);
+            if (e != cudaSuccess) return set_error(NWB_ECUDA, "per-N set-up: %s", cudaGetErrorString(e));
         }
-        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "capture: %s", cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) return set_error(NWB_ECUDA, "instantiate: %s", cudaGetErrorString(ce));
-        return NWB_OK;
+        return capture(0, &graph);
     }
 
     void release_slot(int s) {
@@ -261,6 +320,11 @@ nwb_status nwb_pool_create(size_t hbm_budget_bytes, int max_slots, nwb_precision
     if (e == cudaSuccess) e = cudaMemset(p->d_ntiles, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_counters, sizeof(int) * 8);
     if (e == cudaSuccess) e = cudaMemset(p->d_counters, 0, sizeof(int) * 8);
+    for (int N = 2; N <= 10 && e == cudaSuccess; ++N) {
+        e = cudaStreamCreateWithFlags(&p->side[N], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join_ev[N], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork_ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return bail(set_error(NWB_ECUDA, "nwb_pool_create: %s", cudaGetErrorString(e)));
     *out = p;
@@ -604,13 +668,68 @@ nwb_status nwb_pool_time_steps(nwb_pool* p, int nsteps, float* ms) {
     return r;
 }
 
+nwb_status nwb_pool_set_mode(nwb_pool* p, int mode) {
+    if (!p || (mode != 0 && mode != 1)) return set_error(NWB_EINVAL, "nwb_pool_set_mode: mode must be 0 or 1");
+    NWB_PCU(cudaStreamSynchronize(p->st));
+    if (p->mode != mode) {
+        p->mode = mode;
+        p->drop_graph();
+    }
+    return NWB_OK;
+}
+
+// Times the five stage launches of both modes on the resident cavities (dry
+// stages: a = b = dt = 0, which leaves every state as it is and zeroes the LSRK
+// registers, which the first stage of the next step multiplies by a = 0) and
+// keeps the faster mode.
+nwb_status nwb_pool_autotune(nwb_pool* p, int reps, int* best_mode, float* ms_out /* [2] */) {
+    if (!p || reps < 1) return set_error(NWB_EINVAL, "nwb_pool_autotune: bad argument");
+    float t[2] = {0.f, 0.f};
+    for (int m = 0; m < 2; ++m) {
+        nwb_status r = nwb_pool_set_mode(p, m);
+        if (r == NWB_OK) r = p->ensure_graph();
+        if (r != NWB_OK) return r;
+        cudaGraphExec_t dry = nullptr;
+        r = p->capture(1, &dry);
+        if (r != NWB_OK) return r;
+        cudaEvent_t a, b;
+        NWB_PCU(cudaEventCreate(&a));
+        NWB_PCU(cudaEventCreate(&b));
+        NWB_PCU(cudaGraphLaunch(dry, p->st));  // warm-up
+        NWB_PCU(cudaEventRecord(a, p->st));
+        for (int i = 0; i < reps; ++i) NWB_PCU(cudaGraphLaunch(dry, p->st));
+        NWB_PCU(cudaEventRecord(b, p->st));
+        NWB_PCU(cudaEventSynchronize(b));
+        NWB_PCU(cudaEventElapsedTime(&t[m], a, b));
+        t[m] /= reps;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaGraphExecDestroy(dry);
+        // the dry launches advanced the stage counters of mode 0: reset them
+        NWB_PCU(cudaMemsetAsync(p->d_counters, 0, sizeof(int) * 8, p->st));
+        NWB_PCU(cudaStreamSynchronize(p->st));
+    }
+    const int m = t[1] < t[0] ? 1 : 0;
+    if (best_mode) *best_mode = m;
+    if (ms_out) {
+        ms_out[0] = t[0];
+        ms_out[1] = t[1];
+    }
+    return nwb_pool_set_mode(p, m);
+}
+
 nwb_status nwb_pool_destroy(nwb_pool* p) {
     if (!p) return NWB_OK;
     if (p->st) cudaStreamSynchronize(p->st);
     p->drop_graph();
-    void* ptrs[] = {p->base, p->d_slots, p->d_work, p->d_ntiles, p->d_counters};
+    void* ptrs[] = {p->base, p->d_slots, p->d_work, p->d_work_n, p->d_ntiles, p->d_counters};
     for (void* q : ptrs)
         if (q) cudaFree(q);
+    for (int N = 2; N <= 10; ++N) {
+        if (p->side[N]) cudaStreamDestroy(p->side[N]);
+        if (p->join_ev[N]) cudaEventDestroy(p->join_ev[N]);
+    }
+    if (p->fork_ev) cudaEventDestroy(p->fork_ev);
     if (p->st) cudaStreamDestroy(p->st);
     delete p;
     return NWB_OK;

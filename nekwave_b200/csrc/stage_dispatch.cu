@@ -19,17 +19,17 @@ cudaError_t launch_stage(int N, int geo, int f32, int variant, const StageParams
     }
 }
 
-int stage_variant_count(int N, int geo) {
+int stage_variant_count(int N, int geo, int f32) {
     switch (N) {
-        case 2: return stage_variant_count_n<2>(geo);
-        case 3: return stage_variant_count_n<3>(geo);
-        case 4: return stage_variant_count_n<4>(geo);
-        case 5: return stage_variant_count_n<5>(geo);
-        case 6: return stage_variant_count_n<6>(geo);
-        case 7: return stage_variant_count_n<7>(geo);
-        case 8: return stage_variant_count_n<8>(geo);
-        case 9: return stage_variant_count_n<9>(geo);
-        case 10: return stage_variant_count_n<10>(geo);
+        case 2: return stage_variant_count_n<2>(geo, f32);
+        case 3: return stage_variant_count_n<3>(geo, f32);
+        case 4: return stage_variant_count_n<4>(geo, f32);
+        case 5: return stage_variant_count_n<5>(geo, f32);
+        case 6: return stage_variant_count_n<6>(geo, f32);
+        case 7: return stage_variant_count_n<7>(geo, f32);
+        case 8: return stage_variant_count_n<8>(geo, f32);
+        case 9: return stage_variant_count_n<9>(geo, f32);
+        case 10: return stage_variant_count_n<10>(geo, f32);
         default: return 0;
     }
 }

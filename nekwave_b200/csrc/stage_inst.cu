@@ -1,6 +1,7 @@
 // stage_inst.cu -- instantiations of the fused stage kernel for one N.
 // Compiled once per N (2..10) with -DNWB_N=<N> so the objects build in parallel.
 #include "stage_kernel.cuh"
+#include "stage_mma.cuh"
 #include "stage_variants.h"
 
 #ifndef NWB_N
@@ -18,20 +19,31 @@ namespace stage {
 namespace {
 
 struct Shape {
-    int ks, epb, ksm, minb;
+    int ks, epb, ksm, minb, alg;
 };
-#define NWB_X(ks, epb, ksm, minb) Shape{ks, epb, ksm, minb},
+#define NWB_X(ks, epb, ksm, minb, alg) Shape{ks, epb, ksm, minb, alg},
 constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 #undef NWB_X
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
+constexpr int count_simt() {
+    int n = 0;
+    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg == 0;
+    return n;
+}
+constexpr int kNumSimt = count_simt();
 
 // every variant for the axis-aligned class, variant 0 for the others
 template <int GEO, bool F32, int I>
 cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     if constexpr (I < kNumShapes) {
         if (vid == I) {
-            if constexpr (GEO == GEO_BOX || I == 0) {
-                constexpr Shape v = kShapes[I];
+            constexpr Shape v = kShapes[I];
+            if constexpr (v.alg == 1) {
+                if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
+                    return launch_mma8<v.minb>(p, st, cfg);
+                else
+                    return cudaErrorInvalidValue;
+            } else if constexpr (GEO == GEO_BOX || I == 0) {
                 return launch_cfg<NWB_N, GEO, F32, v.ks, v.epb, (v.ksm != 0), v.minb>(p, st, cfg);
             } else {
                 return cudaErrorInvalidValue;
@@ -44,8 +56,8 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
 }
 
 template <int GEO>
-int count_variants() {
-    return GEO == GEO_BOX ? kNumShapes : 1;
+int count_variants(int f32) {
+    return GEO == GEO_BOX ? (f32 ? kNumSimt : kNumShapes) : 1;
 }
 
 }  // namespace
@@ -71,11 +83,11 @@ cudaError_t launch_stage_n<NWB_N>(int geo, int f32, int variant, const StagePara
 }
 
 template <>
-int stage_variant_count_n<NWB_N>(int geo) {
+int stage_variant_count_n<NWB_N>(int geo, int f32) {
     switch (geo) {
-        case GEO_BOX: return stage::count_variants<GEO_BOX>();
-        case GEO_AFFINE: return stage::count_variants<GEO_AFFINE>();
-        case GEO_NODAL: return stage::count_variants<GEO_NODAL>();
+        case GEO_BOX: return stage::count_variants<GEO_BOX>(f32);
+        case GEO_AFFINE: return stage::count_variants<GEO_AFFINE>(f32);
+        case GEO_NODAL: return stage::count_variants<GEO_NODAL>(f32);
         default: return 0;
     }
 }

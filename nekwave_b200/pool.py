@@ -170,6 +170,18 @@ class CavityPool:
         return dict(used_bytes=used.value, budget_bytes=budget.value, slots_used=n.value,
                     launches=launches.value)
 
+    def set_mode(self, mode: int) -> None:
+        """0: one persistent launch per stage for all N; 1: one launch per N."""
+        check(_lib.lib().nwb_pool_set_mode(self._h, int(mode)))
+
+    def autotune(self, reps: int = 5):
+        """Time both launch modes on the resident cavities, keep the faster;
+        returns (mode, [ms mode 0, ms mode 1])."""
+        best = C.c_int()
+        ms = (C.c_float * 2)()
+        check(_lib.lib().nwb_pool_autotune(self._h, int(reps), C.byref(best), ms))
+        return best.value, [float(ms[0]), float(ms[1])]
+
     def time_steps(self, nsteps: int) -> float:
         ms = C.c_float()
         check(_lib.lib().nwb_pool_time_steps(self._h, int(nsteps), C.byref(ms)))
