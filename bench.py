@@ -17,6 +17,7 @@ maximum over ranks and ``value`` is the sum of all ranks' DOF-stages over it.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -328,8 +329,9 @@ def run_serve(args, rank, world):
     mu = serial_rate / mean_work
     rows = []
     budget = int(float(os.environ.get("NWB_SERVE_BUDGET_GB", "100")) * (1 << 30))
+    base = serving_requests(n, 1.0, seed=args.seed + 100)  # one request set, arrivals at rate 1/s
     for mult in [float(x) for x in args.rates.split(",")]:
-        reqs = serving_requests(n, mult * mu, seed=args.seed + int(mult * 100))
+        reqs = [dataclasses.replace(r, arrival=r.arrival / (mult * mu)) for r in base]
         srv = Server(budget, max_slots=512, precision=args.precision)
         res, wall = srv.run(reqs)
         srv.close()
@@ -337,7 +339,7 @@ def run_serve(args, rank, world):
         rows.append(dict(rate_multiple=mult, rate_per_s=mult * mu, solves_per_s=n / wall,
                          p50_s=st["p50"], p99_s=st["p99"], mean_s=st["mean"],
                          gdof_stage_per_s=sum(r.dof_stages for r in reqs) / wall / 1e9))
-    serial_reqs = serving_requests(n, 1.0 * mu, seed=args.seed + 100)
+    serial_reqs = [dataclasses.replace(r, arrival=r.arrival / mu) for r in base]
     sres, swall = serve_serial(serial_reqs, precision="fp64")
     sst = latency_stats(sres)
     best = max(rows, key=lambda r: r["solves_per_s"])
