@@ -35,6 +35,33 @@ METRIC = "GDOF-stage/s"
 WORKLOAD = dict(workload="periodic_box_32x32x32_N8_central", nel=(32, 32, 32), N=8,
                 periodic=True, c0=0.0, cfl=0.5, sigma=0.1)
 BYTES_PER_DOF_STAGE = 32  # FP64 u and k, each read and written once
+
+
+def workload_spec(name, nel_override, seed):
+    """Single-mesh workloads: c2 (the headline) and c3 (PEC cavity 64x64x32, 6 points,
+    upwind, Gaussian Ex, Ey, Ez with independent seeded centres and widths)."""
+    r = np.random.Generator(np.random.PCG64(seed))
+    if name == "c3":
+        nel = (64, 64, 32) if nel_override == 32 else (2 * nel_override, 2 * nel_override, nel_override)
+        lo, hi = (0.0, 0.0, 0.0), (2.0, 2.0, 1.0)
+        pulses = []
+        for c in range(6):
+            if c < 3:
+                ctr = np.array(lo) + (np.array(hi) - np.array(lo)) * r.uniform(0.25, 0.75, 3)
+                pulses.append((1.0, ctr[0], ctr[1], ctr[2], float(r.uniform(0.05, 0.15))))
+            else:
+                pulses.append((0.0, 0, 0, 0, 0.0))
+        return dict(workload="pec_cavity_64x64x32_N6_upwind" if nel_override == 32 else
+                    f"pec_cavity_{nel[0]}x{nel[1]}x{nel[2]}_N6_upwind", N=6, nel=nel, lo=lo, hi=hi,
+                    periodic=(False, False, False), c0=1.0, flux="upwind", pulses=pulses)
+    nel = (nel_override,) * 3
+    r0 = r.uniform(0.3, 0.7, 3)
+    pulses = [(0.0, 0, 0, 0, 0.0)] * 2 + [(1.0, r0[0], r0[1], r0[2], WORKLOAD["sigma"])] + \
+        [(0.0, 0, 0, 0, 0.0)] * 3
+    return dict(workload=WORKLOAD["workload"] if nel_override == 32 else
+                f"periodic_box_{nel_override}^3_N8_central", N=8, nel=nel, lo=(0.0, 0.0, 0.0),
+                hi=(1.0, 1.0, 1.0), periodic=(True, True, True), c0=0.0, flux="central",
+                pulses=pulses)
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -52,7 +79,7 @@ def parse():
                    help="elements per axis; values other than 32 are for profiling only")
     p.add_argument("--variant", type=int, default=-1,
                    help="stage-kernel launch shape; -1 = autotune on the workload")
-    p.add_argument("--workload", choices=["c2", "batch", "serve"], default="c2",
+    p.add_argument("--workload", choices=["c2", "c3", "batch", "serve"], default="c2",
                    help="c2: periodic 32^3 N=8 (default, the headline); batch: 256 uneven PEC "
                         "cavities in one pool; serve: Poisson request stream")
     p.add_argument("--rates", type=str, default="0.5,1,2",
@@ -144,87 +171,90 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per stage launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
-    try:
-        with open(p) as f:
-            d = json.load(f)
-        return d
-    except (OSError, ValueError):
-        return None
+def profiled_traffic(N):
+    """DRAM bytes per stage launch from the committed ncu summary of the stage kernel
+    with N points per direction, if any (stage_kernel_traffic.json covers N=8,
+    stage_kernel_traffic_n<N>.json the others)."""
+    for name in ("stage_kernel_traffic.json", f"stage_kernel_traffic_n{N}.json"):
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                d = json.load(f)
+        except (OSError, ValueError):
+            continue
+        if int(d.get("N", 8)) == N:
+            return d
+    return None
 
 
 # ---- CPU baseline: the reference's own implementation on the host cores ---------------
-def cpu_reference_rate(seconds_target=15.0, seed=0):
+def _sample_mesh(spec, O):
+    """An 8x8x8-element sub-box of the workload with the same points per direction,
+    boundary kind and flux, built by the reference's own Mesh when available."""
+    N = spec["N"]
+    nel = (8, 8, 8)
+    lo = np.array(spec["lo"])
+    h = (np.array(spec["hi"]) - lo) / np.array(spec["nel"])
+    hi = lo + h * np.array(nel)
+    per = spec["periodic"]
+    if O.ref_available():
+        m = O.ref_box_mesh(N, nel, tuple(lo), tuple(hi), per)
+        return m, m.dxmin_ref, O.ref_step, O.ref().nwref_threads(), "reference"
+    m = O.box_mesh(N, nel, tuple(lo), tuple(hi), per)
+    return m, O.dxmin(m), O.step, O.threads(), "port"
+
+
+def cpu_reference_rate(seconds_target=12.0, spec=None):
     """Times the reference's RHS + LSRK45 (its kernel bodies compiled for the host,
     oracle/_ref) -- or, if that build is absent, the oracle port -- on a bounded sample
-    of the workload: the same element order, flux and pulse on an 8x8x8-element
-    periodic sub-box (1/64 of the mesh), whole LSRK45 steps."""
+    of the workload: whole LSRK45 steps on an 8x8x8-element sub-box with the same
+    points per direction, boundaries and flux."""
     from oracle import oracle as O
-    nel = (8, 8, 8)
-    N = WORKLOAD["N"]
-    kind = "reference" if O.ref_available() else "port"
-    if kind == "reference":
-        m = O.ref_box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
-        dx = m.dxmin_ref
-        stepper = O.ref_step
-        cores = O.ref().nwref_threads()
-    else:
-        m = O.box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
-        dx = O.dxmin(m)
-        stepper = O.step
-        cores = O.threads()
-    u = initial_state(m.x * 4, m.y * 4, m.zc * 4, seed)
+    spec = spec or workload_spec("c2", 32, 0)
+    m, dx, stepper, cores, kind = _sample_mesh(spec, O)
+    u = np.random.Generator(np.random.PCG64(1)).standard_normal(6 * m.npts)
     dt = WORKLOAD["cfl"] * dx
     t0 = time.perf_counter()
-    u, k = stepper(m, WORKLOAD["c0"], dt, 1, u)
+    u, k = stepper(m, spec["c0"], dt, 1, u)
     one = time.perf_counter() - t0
     nsteps = max(1, int(seconds_target / max(one, 1e-3)))
     t0 = time.perf_counter()
-    stepper(m, WORKLOAD["c0"], dt, nsteps, u, k)
+    stepper(m, spec["c0"], dt, nsteps, u, k)
     sec = time.perf_counter() - t0
     dof_stage = 6 * m.npts * 5 * nsteps
     return dict(value=dof_stage / sec / 1e9, unit=METRIC, cores=int(cores), kind=kind,
-                sample=f"{nsteps} LSRK45 steps on an 8x8x8-element periodic sub-box, N=8 "
-                       f"({m.npts} nodes), {sec:.1f} s on {cores} host threads",
+                sample=f"{nsteps} LSRK45 steps on an 8x8x8-element sub-box of the workload, "
+                       f"N={spec['N']} ({m.npts} nodes), {sec:.1f} s on {cores} host threads",
                 seconds=sec, steps=nsteps, npts=m.npts)
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own CPU implementation (oracle/_ref)."""
+    """--impl reference: the reference's own CPU implementation (oracle/_ref), each
+    step one LSRK45 step of an 8x8x8-element sub-box of the workload."""
     if rank != 0:
         return None
     from oracle import oracle as O
-    kind = "reference" if O.ref_available() else "port"
-    N = WORKLOAD["N"]
-    nel = (8, 8, 8)
-    if kind == "reference":
-        m = O.ref_box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
-        dx, stepper, cores = m.dxmin_ref, O.ref_step, O.ref().nwref_threads()
-    else:
-        m = O.box_mesh(N, nel, (0, 0, 0), (0.25, 0.25, 0.25), (True, True, True))
-        dx, stepper, cores = O.dxmin(m), O.step, O.threads()
-    u = initial_state(m.x * 4, m.y * 4, m.zc * 4, args.seed)
+    spec = workload_spec(args.workload if args.workload in ("c2", "c3") else "c2", args.nel, args.seed)
+    m, dx, stepper, cores, kind = _sample_mesh(spec, O)
+    u = np.random.Generator(np.random.PCG64(1)).standard_normal(6 * m.npts)
     k = np.zeros_like(u)
     dt = WORKLOAD["cfl"] * dx
     for _ in range(args.warmup):
-        u, k = stepper(m, WORKLOAD["c0"], dt, 1, u, k)
+        u, k = stepper(m, spec["c0"], dt, 1, u, k)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        u, k = stepper(m, WORKLOAD["c0"], dt, 1, u, k)
+        u, k = stepper(m, spec["c0"], dt, 1, u, k)
         times.append(time.perf_counter() - t0)
     sec = sum(times)
     value = 6 * m.npts * 5 * args.steps / sec / 1e9
-    sample = (f"each step: one LSRK45 step on an 8x8x8-element periodic sub-box of the "
-              f"workload, N=8 ({m.npts} nodes)")
+    sample = (f"each step: one LSRK45 step on an 8x8x8-element sub-box of the workload, "
+              f"N={spec['N']} ({m.npts} nodes)")
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload=WORKLOAD["workload"], N=N, nel=list(WORKLOAD["nel"]),
-                           flux="central", cfl=WORKLOAD["cfl"], sample_nel=list(nel)),
+            "config": dict(workload=spec["workload"], N=spec["N"], nel=list(spec["nel"]),
+                           flux=spec["flux"], cfl=WORKLOAD["cfl"], sample_nel=[8, 8, 8]),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": int(cores), "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
@@ -389,17 +419,14 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    N = WORKLOAD["N"]
-    nel = (args.nel,) * 3
+    spec = workload_spec(args.workload, args.nel, args.seed + rank)
+    N, nel = spec["N"], spec["nel"]
     npts = nel[0] * nel[1] * nel[2] * N ** 3
     from nekwave_b200.workloads import box_dxmin
-    dt = WORKLOAD["cfl"] * box_dxmin(N, nel, (0, 0, 0), (1, 1, 1))
-    r0 = np.random.Generator(np.random.PCG64(args.seed + rank)).uniform(0.3, 0.7, 3)
-    pulses = [(0.0, 0, 0, 0, 0.0)] * 2 + [(1.0, r0[0], r0[1], r0[2], WORKLOAD["sigma"])] + \
-        [(0.0, 0, 0, 0, 0.0)] * 3
+    dt = WORKLOAD["cfl"] * box_dxmin(N, nel, spec["lo"], spec["hi"])
+    pulses = spec["pulses"]
     solver = DgSolver(args.precision)
-    solver.initializeBox(N, nel, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), WORKLOAD["c0"],
-                         periodic=(True, True, True))
+    solver.initializeBox(N, nel, spec["lo"], spec["hi"], spec["c0"], periodic=spec["periodic"])
     solver.initPulse(pulses)
     u0 = solver.downloadState()
     tune_ms = None
@@ -420,7 +447,7 @@ def main():
         solver.finalize()
         return
 
-    # ---- timed region: K steps, inputs resident in HBM (3 x 805 MB > L2) ---------------
+    # ---- timed region: K steps, inputs resident in HBM (u_in, u_out, k each > L2) -------
     launches0 = solver.launchCount()
     with ClockSampler(local) as clk:
         barrier()
@@ -440,7 +467,7 @@ def main():
     alg_bytes = BYTES_PER_DOF_STAGE * 6 * npts
     achieved = alg_bytes / (stage_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    tr = profiled_traffic()
+    tr = profiled_traffic(N)
     traffic = None
     if tr and tr.get("npts") and tr.get("precision", "fp64") == args.precision:
         traffic = tr["dram_bytes_per_launch"] * npts / tr["npts"]
@@ -471,8 +498,7 @@ def main():
         out = {}
         for prec in ("fp64", "fp32"):
             a = DgSolver(prec)
-            a.initializeBox(N, nel, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), WORKLOAD["c0"],
-                            periodic=(True, True, True))
+            a.initializeBox(N, nel, spec["lo"], spec["hi"], spec["c0"], periodic=spec["periodic"])
             a.initPulse(pulses)
             e0 = a.energy()
             a.steps(dt, args.accuracy_steps)
@@ -486,7 +512,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_rate()
+        cpu = cpu_reference_rate(spec=spec)
 
     if dist_on:
         dist.barrier()
@@ -498,12 +524,11 @@ def main():
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
             "data": "synthetic (seeded Gaussian pulse)",
-            "config": dict(workload=WORKLOAD["workload"] if args.nel == 32 else
-                           f"periodic_box_{args.nel}^3_N8_central", N=N, order=N - 1,
+            "config": dict(workload=spec["workload"], N=N, order=N - 1,
                            nel=list(nel), npts=npts, dof=6 * npts,
-                           flux="central", cfl=WORKLOAD["cfl"], dt=dt,
+                           flux=spec["flux"], cfl=WORKLOAD["cfl"], dt=dt,
                            precision=args.precision, parallelism=f"replicas x{world}",
-                           l2="inputs larger than L2 (u_in, u_out, k: 3 x 805 MB)",
+                           l2="inputs larger than L2 (u_in, u_out, k: 3 x %.0f MB)" % (npts * 48 / 1e6),
                            kernel=dict(variant=info["variant"], ks=info["ks"], epb=info["epb"],
                                        k_in_smem=info["ksmem"], minb=info["minb"],
                                        threads=info["threads_per_block"],
