@@ -9,6 +9,7 @@
 // launch, so each result is bit-identical alone and in any mix.
 #include "batch.cuh"
 #include "stage_kernel.cuh"
+#include "stage_pipe.cuh"
 
 namespace nwb {
 namespace {
@@ -17,27 +18,60 @@ using stage::SmemLayout;
 using stage::stage_tile;
 
 // Shape per N for the batch kernel's blocks (kBatchThreads = 128): KS threads
-// per column, EPB elements -- the single-mesh kernel's fastest shapes that fit.
+// per column, EPB elements, ALG the kernel family -- the single-mesh default's
+// family and arithmetic for each N (stage_variants.h entry 0), in a shape that
+// fits, so a cavity in the pool evolves bit for bit as it does alone.
 template <int N> struct BShape;
-template <> struct BShape<2> { static constexpr int KS = 2, EPB = 16; };
-template <> struct BShape<3> { static constexpr int KS = 1, EPB = 14; };
-template <> struct BShape<4> { static constexpr int KS = 1, EPB = 8; };
-template <> struct BShape<5> { static constexpr int KS = 1, EPB = 4; };
-template <> struct BShape<6> { static constexpr int KS = 3, EPB = 1; };
-template <> struct BShape<7> { static constexpr int KS = 1, EPB = 2; };
-template <> struct BShape<8> { static constexpr int KS = 2, EPB = 1; };
-template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1; };
-template <> struct BShape<10> { static constexpr int KS = 1, EPB = 1; };
+template <> struct BShape<2> { static constexpr int KS = 2, EPB = 16, ALG = 0; };
+template <> struct BShape<3> { static constexpr int KS = 1, EPB = 14, ALG = 0; };
+template <> struct BShape<4> { static constexpr int KS = 2, EPB = 4, ALG = 4; };
+template <> struct BShape<5> { static constexpr int KS = 2, EPB = 2, ALG = 4; };
+template <> struct BShape<6> { static constexpr int KS = 2, EPB = 1, ALG = 4; };
+template <> struct BShape<7> { static constexpr int KS = 2, EPB = 1, ALG = 4; };
+template <> struct BShape<8> { static constexpr int KS = 2, EPB = 1, ALG = 8; };
+template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1, ALG = 0; };
+template <> struct BShape<10> { static constexpr int KS = 1, EPB = 1, ALG = 0; };
 
 template <int N, bool F32>
 constexpr int bsmem() {
-    return SmemLayout<N, F32, BShape<N>::EPB, false>::total;
+    using B = BShape<N>;
+    if constexpr (B::ALG == 0) return SmemLayout<N, F32, B::EPB, false>::total;
+    else return stage::Layout2<N, F32, B::EPB, false, (((B::ALG - 2) & 4) != 0)>::total;
+}
+
+// One tile of the second family without the persistent loop: stage u_in (and D,
+// geometry, connections), wait, compute.  Threads beyond the shape's count take
+// part in the barriers only.
+template <int N, bool F32, int KS, int EPB, int ALG>
+__device__ __forceinline__ void tile2(const StageParams& P, int e0, unsigned char* smem, int tid) {
+    constexpr bool SPLIT = ((ALG - 2) & 2) != 0, PAD = ((ALG - 2) & 4) != 0;
+    static_assert(((ALG - 2) & 1) == 0, "one tile per call");
+    using L2 = stage::Layout2<N, F32, EPB, false, PAD>;
+    constexpr int NT = EPB * KS * N * N;
+    double* sD = reinterpret_cast<double*>(smem + L2::D);
+    double* su = reinterpret_cast<double*>(smem + L2::u0);
+    ElemGeo* sg = reinterpret_cast<ElemGeo*>(smem + L2::geo0);
+    int* sc = reinterpret_cast<int*>(smem + L2::conn0);
+    if (tid < NT) {
+        for (int x = tid; x < N * N; x += NT) stage::cp_async8(sD + x, P.D + x);
+        stage::issue2<N, GEO_BOX, EPB, NT, PAD>(P, e0, su, sg, sc, tid);
+    }
+    stage::cp_async_commit();
+    stage::cp_async_wait<0>();
+    __syncthreads();
+    stage::compute2<N, GEO_BOX, F32, KS, EPB, SPLIT, PAD>(P, e0, su, sg, sc, sD,
+                                                          reinterpret_cast<double*>(smem + L2::flux),
+                                                          smem + L2::uc, tid);
 }
 
 template <int N, bool F32>
 __device__ __forceinline__ void run_tile(const StageParams& P, int e0, unsigned char* smem, int tid) {
-    static_assert(BShape<N>::KS * BShape<N>::EPB * N * N <= kBatchThreads, "shape too large");
-    stage_tile<N, GEO_BOX, F32, BShape<N>::KS, BShape<N>::EPB, false, false>(P, e0, smem, tid);
+    using B = BShape<N>;
+    static_assert(B::KS * B::EPB * N * N <= kBatchThreads, "shape too large");
+    if constexpr (B::ALG == 0)
+        stage_tile<N, GEO_BOX, F32, B::KS, B::EPB, false, false>(P, e0, smem, tid);
+    else
+        tile2<N, F32, B::KS, B::EPB, B::ALG>(P, e0, smem, tid);
 }
 
 // Carpenter-Kennedy LSRK45 (src/dg_solver.cpp:58-69).
@@ -129,8 +163,10 @@ __device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, 
 }
 
 // One block per tile of one N: the single-mesh kernel's tuned shape for that N,
-// fully unrolled, reading its slot from the work item (per-N mode).
-template <int N, bool F32, int KS, int EPB, bool KSMEM, int MINB>
+// fully unrolled, reading its slot from the work item (per-N mode).  ALG 0 is the
+// first-family tile (stage_kernel.cuh); ALG 2 + flags (SPLIT = 2, PAD = 4, no
+// PIPE: the work list is walked one tile per block) the second (stage_pipe.cuh).
+template <int N, bool F32, int KS, int EPB, bool KSMEM, int MINB, int ALG>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
 batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
                      int stage, int dry) {
@@ -139,28 +175,34 @@ batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restri
     const SlotDev& S = slots[w.slot];
     if (!S.active) return;
     const StageParams P = slot_params(S, stage, dry);
-    stage_tile<N, GEO_BOX, F32, KS, EPB, KSMEM, true>(P, w.e0, smem, threadIdx.x);
+    if constexpr (ALG == 0)
+        stage_tile<N, GEO_BOX, F32, KS, EPB, KSMEM, true>(P, w.e0, smem, threadIdx.x);
+    else
+        tile2<N, F32, KS, EPB, ALG>(P, w.e0, smem, threadIdx.x);
 }
 
-// Per-N shapes of the per-N mode: the single-mesh defaults (stage_variants.h entry 0).
+// Per-N shapes of the per-N mode: the single-mesh defaults (stage_variants.h entry
+// 0), with the persistent form of N = 4 replaced by its one-tile-per-block form.
 template <int N> struct NShape;
-template <> struct NShape<2> { static constexpr int KS = 2, EPB = 16, KSM = 1, MINB = 1; };
-template <> struct NShape<3> { static constexpr int KS = 1, EPB = 16, KSM = 0, MINB = 4; };
-template <> struct NShape<4> { static constexpr int KS = 1, EPB = 8, KSM = 0, MINB = 4; };
-template <> struct NShape<5> { static constexpr int KS = 1, EPB = 4, KSM = 0, MINB = 4; };
-template <> struct NShape<6> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 3; };
-template <> struct NShape<7> { static constexpr int KS = 1, EPB = 2, KSM = 0, MINB = 3; };
-template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4; };
-template <> struct NShape<9> { static constexpr int KS = 3, EPB = 1, KSM = 0, MINB = 2; };
-template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2; };
+template <> struct NShape<2> { static constexpr int KS = 2, EPB = 16, KSM = 1, MINB = 1, ALG = 0; };
+template <> struct NShape<3> { static constexpr int KS = 1, EPB = 16, KSM = 0, MINB = 4, ALG = 0; };
+template <> struct NShape<4> { static constexpr int KS = 2, EPB = 4, KSM = 0, MINB = 4, ALG = 4; };
+template <> struct NShape<5> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 4, ALG = 4; };
+template <> struct NShape<6> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 3, ALG = 4; };
+template <> struct NShape<7> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 4; };
+template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 8; };
+template <> struct NShape<9> { static constexpr int KS = 3, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
+template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
 
 template <int N, bool F32>
 cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
                      cudaStream_t st, int* epb_out) {
     using Sh = NShape<N>;
     constexpr int threads = Sh::EPB * Sh::KS * N * N;
-    constexpr int smem = SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total;
-    auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB>;
+    constexpr int smem = Sh::ALG == 0
+        ? SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total
+        : stage::Layout2<N, F32, Sh::EPB, false, (((Sh::ALG - 2) & 4) != 0)>::total;
+    auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB, Sh::ALG>;
     if (epb_out) *epb_out = Sh::EPB;
     static bool attr_set = false;
     if (!attr_set) {

@@ -2,6 +2,7 @@
 // Compiled once per N (2..10) with -DNWB_N=<N> so the objects build in parallel.
 #include "stage_kernel.cuh"
 #include "stage_mma.cuh"
+#include "stage_pipe.cuh"
 #include "stage_variants.h"
 
 #ifndef NWB_N
@@ -27,10 +28,10 @@ constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
 constexpr int count_simt() {
     int n = 0;
-    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg == 0;
+    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1;
     return n;
 }
-constexpr int kNumSimt = count_simt();
+constexpr int kNumSimt = count_simt();  // every variant but the FP64 tensor-core ones (last)
 
 // every variant for the axis-aligned class, variant 0 for the others
 template <int GEO, bool F32, int I>
@@ -41,6 +42,14 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
             if constexpr (v.alg == 1) {
                 if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
                     return launch_mma8<v.minb>(p, st, cfg);
+                else
+                    return cudaErrorInvalidValue;
+            } else if constexpr (v.alg >= 2) {
+                static_assert(v.ksm == 0 && v.alg <= 9, "second family: k from L2, flags 0..7");
+                constexpr int fl = v.alg - 2;
+                if constexpr (GEO == GEO_BOX || I == 0)
+                    return launch2<NWB_N, GEO, F32, v.ks, v.epb, v.minb, (fl & 1) != 0, (fl & 2) != 0,
+                                   (fl & 4) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == 0) {

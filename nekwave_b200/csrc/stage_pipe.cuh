@@ -1,0 +1,543 @@
+// stage_pipe.cuh -- second family of fused stage kernels.
+//
+// Same arithmetic as stage_tile (stage_kernel.cuh): per element the volume curl,
+// the numerical flux with its lift, and the LSRK45 update, each residual entry
+// formed once in a fixed order.  Three independent options change the schedule
+// and the shared-memory traffic:
+//
+//   PIPE   the block stays resident and walks the tiles t = blockIdx.x,
+//          blockIdx.x + gridDim.x, ...; while it computes tile t, the asynchronous
+//          copies of its next tile (u_in, per-element geometry and connections) are
+//          in flight into a second buffer and that tile's k lines are being pulled
+//          into L2.  Without PIPE a block computes one tile, as stage_tile does.
+//   SPLIT  (KS = 2) the two threads of a node column split the residual by field
+//          instead of by planes: thread h = 0 forms the E residual (curl H) and
+//          h = 1 the H residual (-curl E), each for all N planes.  The components
+//          a thread differentiates along t are read once per column into
+//          registers, so shared memory serves only the r and s derivatives, and
+//          each thread lifts, updates and stores three components.
+//   PAD    rows of the shared-memory tile are N+1 doubles apart (node (i,j,k) of
+//          an element at i + (N+1)(j + N k)), which spreads the traces of the
+//          r-faces (i = 0, N-1) and the rows of the r-derivative over the banks.
+//
+// In every form the face phase requests the neighbour values of all of a thread's
+// face points before it forms any flux, and each node's k is read before the
+// derivative sums that hide its latency.
+#pragma once
+#include "stage_kernel.cuh"
+
+namespace nwb {
+namespace stage {
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+// Shared-memory index of local node n = i + N j + N^2 k of a tile (element-major).
+template <int N, bool PAD>
+__device__ __forceinline__ int pidx(int n) {
+    if constexpr (PAD) return n + n / N;
+    else return n;
+}
+
+template <int N, bool F32, int EPB, bool PIPE, bool PAD>
+struct Layout2 {
+    static constexpr int N2 = N * N, N3 = N2 * N;
+    static constexpr int EN3 = PAD ? N2 * (N + 1) : N3;                  // element stride
+    static constexpr int CS = EPB * EN3;                                  // component stride
+    static constexpr int NB = PIPE ? 2 : 1;                               // buffers
+    static constexpr int tile = 6 * CS * 8;
+    static constexpr int geo_b = EPB * static_cast<int>(sizeof(ElemGeo));
+    static constexpr int conn_b = align16(EPB * 6 * 4);
+    static constexpr int u0 = 0;
+    static constexpr int geo0 = u0 + NB * tile;
+    static constexpr int conn0 = geo0 + NB * geo_b;
+    static constexpr int D = conn0 + NB * conn_b;
+    static constexpr int flux = D + align16(N2 * 8);
+    static constexpr int uc = flux + EPB * 36 * N2 * 8;
+    static constexpr int total = uc + (F32 ? align16(6 * CS * 4) : 0);
+    static_assert(tile % 16 == 0 && geo_b % 16 == 0, "16-byte aligned buffers");
+};
+
+// Asynchronous copies of the tile that starts at element e0 into one buffer set.
+// Unpadded even N: the tile and every component start on a 16-byte boundary
+// (e0*N^3*8 and stride*8 are multiples of 16), so the copies move 16 bytes each.
+template <int N, int GEO, int EPB, int NT, bool PAD>
+__device__ __forceinline__ void issue2(const StageParams& P, const int e0, double* su, ElemGeo* sg,
+                                       int* sc, const int tid) {
+    constexpr int N3 = N * N * N;
+    constexpr int CS = EPB * (PAD ? N * N * (N + 1) : N3);
+    const int nvalid = min(EPB, P.nelt - e0);
+    const long long gbase = static_cast<long long>(e0) * N3;
+    const long long S = P.stride;
+    const int cnt = nvalid * N3;
+    if constexpr (N % 2 == 0 && !PAD) {
+        const int c2 = cnt / 2;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double* src = P.u_in + c * S + gbase;
+            double* dst = su + c * CS;
+            for (int x = tid; x < c2; x += NT) cp_async16(dst + 2 * x, src + 2 * x);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double* src = P.u_in + c * S + gbase;
+            double* dst = su + c * CS;
+            for (int x = tid; x < cnt; x += NT) cp_async8(dst + pidx<N, PAD>(x), src + x);
+        }
+    }
+    if constexpr (GEO != GEO_NODAL) {
+        constexpr int chunks = static_cast<int>(sizeof(ElemGeo) / 16);
+        const char* gsrc = reinterpret_cast<const char*>(P.geo + e0);
+        char* gdst = reinterpret_cast<char*>(sg);
+        for (int x = tid; x < nvalid * chunks; x += NT) cp_async16(gdst + 16 * x, gsrc + 16 * x);
+        for (int x = tid; x < nvalid * 6; x += NT) cp_async4(sc + x, P.conn + e0 * 6 + x);
+    }
+    // the tile's k lines into L2; the owner threads read them in the column phase
+    const int lines = (cnt * 8 + 127) / 128;
+    for (int x = tid; x < 6 * lines; x += NT) {
+        const int c = x / lines, ln = x - c * lines;
+        const double* a = P.k + c * S + gbase + ln * 16;
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a));
+    }
+}
+
+// Lifted face terms of node (i,j,k) for the NC components starting at c0, added
+// in the reference's face order 0..5.
+template <int N, int NC>
+__device__ __forceinline__ void add_lifts(const double* Fl, int c0, int i, int j, int k, double* rhs) {
+    constexpr int N2 = N * N;
+    if (j == 0) {
+        const double* F = Fl + 0 * 6 * N2 + (i + N * k) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+    if (i == N - 1) {
+        const double* F = Fl + 1 * 6 * N2 + (j + N * k) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+    if (j == N - 1) {
+        const double* F = Fl + 2 * 6 * N2 + (i + N * k) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+    if (i == 0) {
+        const double* F = Fl + 3 * 6 * N2 + (j + N * k) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+    if (k == 0) {
+        const double* F = Fl + 4 * 6 * N2 + (i + N * j) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+    if (k == N - 1) {
+        const double* F = Fl + 5 * 6 * N2 + (i + N * j) + c0 * N2;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rhs[c] += F[c * N2];
+    }
+}
+
+// Face phase and column phase of one tile whose u_in, geometry and connections
+// are resident in (su, sg, sc).  All threads of the block call it; threads
+// tid >= EPB*KS*N*N take part in the barrier only.
+template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD>
+__device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
+                                         const ElemGeo* sg, const int* sc, const double* sD,
+                                         double* sflux, unsigned char* smem_uc, const int tid) {
+    using TC = typename std::conditional<F32, float, double>::type;
+    constexpr int N2 = N * N, N3 = N2 * N;
+    constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
+    constexpr int PP = RP * N;                       // plane pitch
+    constexpr int EN3 = PP * N;                      // element stride
+    constexpr int TPE = KS * N2;
+    constexpr int NT = EPB * TPE;
+    constexpr int KPT = (N + KS - 1) / KS;
+    constexpr int CS = EPB * EN3;
+    constexpr int FPT = (6 * N2 + TPE - 1) / TPE;    // face points per thread
+    static_assert(!SPLIT || KS == 2, "the field split needs two threads per column");
+
+    const int team = tid / TPE;
+    const int lt = tid - team * TPE;
+    const int loc = lt % N2;
+    const int h = lt / N2;
+    const int i = loc % N;
+    const int j = loc / N;
+    const int nvalid = min(EPB, P.nelt - e0);
+    const int e = e0 + team;
+    const bool active = team < nvalid;
+    const long long S = P.stride;
+
+    const TC* s_uc;
+    if constexpr (F32) {
+        // FP32 copy of the tile as deviations from the element's centre node: the
+        // derivatives are unchanged (rows of D sum to zero) and the rounding error
+        // scales with the variation across the element instead of |u|
+        TC* w = reinterpret_cast<TC*>(smem_uc);
+        constexpr int centre = (N / 2) * (1 + RP + PP);
+        const int cnt = tid < NT ? nvalid * EN3 : 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            for (int x = tid; x < cnt; x += NT) {
+                const double ref = su[c * CS + (x / EN3) * EN3 + centre];
+                w[c * CS + x] = static_cast<float>(su[c * CS + x] - ref);
+            }
+        s_uc = w;
+    } else {
+        s_uc = reinterpret_cast<const TC*>(su);
+    }
+
+    // ---- face phase: neighbour values of all of this thread's face points are
+    // requested first, then the fluxes are formed
+    if (active) {
+        const double* U = su + team * EN3;
+        double nb[FPT][6];
+        long long vBs[FPT];
+#pragma unroll
+        for (int q = 0; q < FPT; ++q) {
+            const int fp = lt + q * TPE;
+            long long vB = -1;
+            if (fp < 6 * N2) {
+                const int f = fp / N2;
+                const int pq = fp - f * N2;
+                const int p = pq % N, qq = pq / N;
+                if constexpr (GEO == GEO_NODAL) {
+                    vB = P.fplus[(static_cast<long long>(e) * 6 + f) * N2 + pq];
+                } else {
+                    const int cd = sc[team * 6 + f];
+                    if (cd != kConnPEC) {
+                        const int eB = cd >> 6, fB = (cd >> 3) & 7, o = cd & 7;
+                        int a = (o & 4) ? qq : p;
+                        int b = (o & 4) ? p : qq;
+                        if (o & 1) a = N - 1 - a;
+                        if (o & 2) b = N - 1 - b;
+                        vB = static_cast<long long>(eB) * N3 + face_local<N>(fB, a, b);
+                    }
+                }
+                if (vB >= 0) {
+                    const long long eB = vB / N3;
+                    if (eB >= e0 && eB < e0 + nvalid) {
+                        const int el = static_cast<int>(eB - e0);
+                        const int sidx = el * EN3 + pidx<N, PAD>(static_cast<int>(vB - eB * N3));
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) nb[q][c] = su[c * CS + sidx];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) nb[q][c] = __ldg(P.u_in + c * S + vB);
+                    }
+                }
+            }
+            vBs[q] = vB;
+        }
+#pragma unroll
+        for (int q = 0; q < FPT; ++q) {
+            const int fp = lt + q * TPE;
+            if (fp >= 6 * N2) break;
+            const int f = fp / N2;
+            const int pq = fp - f * N2;
+            const int p = pq % N, qq = pq / N;
+            const int m = pidx<N, PAD>(face_local<N>(f, p, qq));
+            const double Exm = U[0 * CS + m], Eym = U[1 * CS + m], Ezm = U[2 * CS + m];
+            const double Hxm = U[3 * CS + m], Hym = U[4 * CS + m], Hzm = U[5 * CS + m];
+            double nxd, nyd, nzd, lift;
+            if constexpr (GEO == GEO_NODAL) {
+                const long long g = (static_cast<long long>(e) * 6 + f) * N2 + pq;
+                nxd = P.fnrm[g];
+                nyd = P.fnrm[P.nfp + g];
+                nzd = P.fnrm[2 * P.nfp + g];
+                lift = P.flift[g];
+            } else {
+                const ElemGeo& G = sg[team];
+                nxd = G.nrm[f][0];
+                nyd = G.nrm[f][1];
+                nzd = G.nrm[f][2];
+                lift = G.lift[f];
+            }
+            double jmp[6];
+            if (vBs[q] < 0) {
+                // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
+                jmp[0] = -2.0 * Exm; jmp[1] = -2.0 * Eym; jmp[2] = -2.0 * Ezm;
+                jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+            } else {
+                jmp[0] = nb[q][0] - Exm; jmp[1] = nb[q][1] - Eym; jmp[2] = nb[q][2] - Ezm;
+                jmp[3] = nb[q][3] - Hxm; jmp[4] = nb[q][4] - Hym; jmp[5] = nb[q][5] - Hzm;
+            }
+            TC fl[6];
+            numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
+                               static_cast<TC>(0.5 * P.c0), static_cast<TC>(jmp[0]),
+                               static_cast<TC>(jmp[1]), static_cast<TC>(jmp[2]),
+                               static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
+                               static_cast<TC>(jmp[5]), fl);
+            double* F = sflux + (team * 6 + f) * 6 * N2 + pq;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
+        }
+    }
+    __syncthreads();
+
+    // ---- column phase: volume curl + face terms + LSRK update ------------------
+    if (!active) return;
+    const TC* U = s_uc + team * EN3;
+    const double* Uf = su + team * EN3;
+    const double* Fl = sflux + team * 36 * N2;
+    TC Dr[N], Ds[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        Dr[l] = static_cast<TC>(sD[i + l * N]);
+        Ds[l] = static_cast<TC>(sD[j + l * N]);
+    }
+    TC m_[9];
+    if constexpr (GEO != GEO_NODAL) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) m_[c] = static_cast<TC>(sg[team].met[c]);
+    }
+    const double A = P.a, B = P.b, DT = P.dt;
+    const long long ebase = static_cast<long long>(e) * N3;
+
+    if constexpr (SPLIT) {
+        // thread h = 0: E residual from V = H (+curl H); h = 1: H residual from V = E (-curl E)
+        const int src = h == 0 ? 3 : 0;
+        const int dst = 3 - src;
+        const double sgn = h == 0 ? 1.0 : -1.0;
+        const TC* V = U + src * CS;
+        constexpr int NC = GEO == GEO_BOX ? 2 : 3;  // components differentiated along t
+        TC col[NC][N];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int l = 0; l < N; ++l) col[c][l] = V[c * CS + i + RP * j + PP * l];
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            const int mn = i + N * j + N2 * k;           // node in natural numbering
+            const int ms = i + RP * j + PP * k;          // node in shared memory
+            const long long g = ebase + mn;
+            double kold[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) kold[c] = __ldcg(P.k + (dst + c) * S + g);
+            double rhs[3];
+            if constexpr (GEO == GEO_BOX) {
+                TC Vz_r = 0, Vy_r = 0, Vz_s = 0, Vx_s = 0, Vy_t = 0, Vx_t = 0;
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const int ir = PP * k + RP * j + l;
+                    const int is = PP * k + RP * l + i;
+                    Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
+                    Vz_s += ds * V[2 * CS + is]; Vx_s += ds * V[0 * CS + is];
+                    Vy_t += dt * col[1][l]; Vx_t += dt * col[0][l];
+                }
+                const TC rx = m_[0], sy = m_[4], tz = m_[8];
+                rhs[0] = sgn * static_cast<double>(sy * Vz_s - tz * Vy_t);
+                rhs[1] = sgn * static_cast<double>(tz * Vx_t - rx * Vz_r);
+                rhs[2] = sgn * static_cast<double>(rx * Vy_r - sy * Vx_s);
+            } else {
+                TC dr_[3] = {0, 0, 0}, ds_[3] = {0, 0, 0}, dt_[3] = {0, 0, 0};
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const int ir = PP * k + RP * j + l;
+                    const int is = PP * k + RP * l + i;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        dr_[c] += dr * V[c * CS + ir];
+                        ds_[c] += ds * V[c * CS + is];
+                        dt_[c] += dt * col[c][l];
+                    }
+                }
+                TC rx, sx, tx, ry, sy, ty, rz, sz, tz;
+                if constexpr (GEO == GEO_NODAL) {
+                    rx = static_cast<TC>(P.met_n[0 * S + g]); sx = static_cast<TC>(P.met_n[1 * S + g]);
+                    tx = static_cast<TC>(P.met_n[2 * S + g]); ry = static_cast<TC>(P.met_n[3 * S + g]);
+                    sy = static_cast<TC>(P.met_n[4 * S + g]); ty = static_cast<TC>(P.met_n[5 * S + g]);
+                    rz = static_cast<TC>(P.met_n[6 * S + g]); sz = static_cast<TC>(P.met_n[7 * S + g]);
+                    tz = static_cast<TC>(P.met_n[8 * S + g]);
+                } else {
+                    rx = m_[0]; sx = m_[1]; tx = m_[2]; ry = m_[3]; sy = m_[4];
+                    ty = m_[5]; rz = m_[6]; sz = m_[7]; tz = m_[8];
+                }
+                // physical curl, src/device/dg_kernels.cu:140-149
+                const TC c1 = (dr_[2] * ry + ds_[2] * sy + dt_[2] * ty) - (dr_[1] * rz + ds_[1] * sz + dt_[1] * tz);
+                const TC c2 = (dr_[0] * rz + ds_[0] * sz + dt_[0] * tz) - (dr_[2] * rx + ds_[2] * sx + dt_[2] * tx);
+                const TC c3 = (dr_[1] * rx + ds_[1] * sx + dt_[1] * tx) - (dr_[0] * ry + ds_[0] * sy + dt_[0] * ty);
+                rhs[0] = sgn * static_cast<double>(c1);
+                rhs[1] = sgn * static_cast<double>(c2);
+                rhs[2] = sgn * static_cast<double>(c3);
+            }
+            add_lifts<N, 3>(Fl, dst, i, j, k, rhs);
+            // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double kn = A * kold[c] + DT * rhs[c];
+                __stcs(P.k + (dst + c) * S + g, kn);
+                __stcs(P.u_out + (dst + c) * S + g, Uf[(dst + c) * CS + ms] + B * kn);
+            }
+        }
+    } else {
+        // one plane at a time: the register budget goes to the batched loads
+#pragma unroll 1
+        for (int kk = 0; kk < KPT; ++kk) {
+            const int k = h * KPT + kk;
+            if (KS > 1 && k >= N) break;
+            const int mn = i + N * j + N2 * k;
+            const int ms = i + RP * j + PP * k;
+            const long long g = ebase + mn;
+            double kold[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) kold[c] = __ldcg(P.k + c * S + g);
+            double rhs[6];
+            if constexpr (GEO == GEO_BOX) {
+                TC Hz_r = 0, Hy_r = 0, Ez_r = 0, Ey_r = 0;
+                TC Hz_s = 0, Hx_s = 0, Ez_s = 0, Ex_s = 0;
+                TC Hy_t = 0, Hx_t = 0, Ey_t = 0, Ex_t = 0;
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const int ir = PP * k + RP * j + l;
+                    const int is = PP * k + RP * l + i;
+                    const int it = PP * l + RP * j + i;
+                    Hz_r += dr * U[5 * CS + ir]; Hy_r += dr * U[4 * CS + ir];
+                    Ez_r += dr * U[2 * CS + ir]; Ey_r += dr * U[1 * CS + ir];
+                    Hz_s += ds * U[5 * CS + is]; Hx_s += ds * U[3 * CS + is];
+                    Ez_s += ds * U[2 * CS + is]; Ex_s += ds * U[0 * CS + is];
+                    Hy_t += dt * U[4 * CS + it]; Hx_t += dt * U[3 * CS + it];
+                    Ey_t += dt * U[1 * CS + it]; Ex_t += dt * U[0 * CS + it];
+                }
+                const TC rx = m_[0], sy = m_[4], tz = m_[8];
+                rhs[0] = static_cast<double>(sy * Hz_s - tz * Hy_t);
+                rhs[1] = static_cast<double>(tz * Hx_t - rx * Hz_r);
+                rhs[2] = static_cast<double>(rx * Hy_r - sy * Hx_s);
+                rhs[3] = static_cast<double>(tz * Ey_t - sy * Ez_s);
+                rhs[4] = static_cast<double>(rx * Ez_r - tz * Ex_t);
+                rhs[5] = static_cast<double>(sy * Ex_s - rx * Ey_r);
+            } else {
+                TC dr_[6] = {0, 0, 0, 0, 0, 0}, ds_[6] = {0, 0, 0, 0, 0, 0}, dt_[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const int ir = PP * k + RP * j + l;
+                    const int is = PP * k + RP * l + i;
+                    const int it = PP * l + RP * j + i;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        dr_[c] += dr * U[c * CS + ir];
+                        ds_[c] += ds * U[c * CS + is];
+                        dt_[c] += dt * U[c * CS + it];
+                    }
+                }
+                TC rx, sx, tx, ry, sy, ty, rz, sz, tz;
+                if constexpr (GEO == GEO_NODAL) {
+                    rx = static_cast<TC>(P.met_n[0 * S + g]); sx = static_cast<TC>(P.met_n[1 * S + g]);
+                    tx = static_cast<TC>(P.met_n[2 * S + g]); ry = static_cast<TC>(P.met_n[3 * S + g]);
+                    sy = static_cast<TC>(P.met_n[4 * S + g]); ty = static_cast<TC>(P.met_n[5 * S + g]);
+                    rz = static_cast<TC>(P.met_n[6 * S + g]); sz = static_cast<TC>(P.met_n[7 * S + g]);
+                    tz = static_cast<TC>(P.met_n[8 * S + g]);
+                } else {
+                    rx = m_[0]; sx = m_[1]; tx = m_[2]; ry = m_[3]; sy = m_[4];
+                    ty = m_[5]; rz = m_[6]; sz = m_[7]; tz = m_[8];
+                }
+                // physical curl, src/device/dg_kernels.cu:140-149
+#pragma unroll
+                for (int fld = 0; fld < 2; ++fld) {
+                    const int o = fld == 0 ? 3 : 0;
+                    const TC u1r = dr_[o], u1s = ds_[o], u1t = dt_[o];
+                    const TC u2r = dr_[o + 1], u2s = ds_[o + 1], u2t = dt_[o + 1];
+                    const TC u3r = dr_[o + 2], u3s = ds_[o + 2], u3t = dt_[o + 2];
+                    const TC c1 = (u3r * ry + u3s * sy + u3t * ty) - (u2r * rz + u2s * sz + u2t * tz);
+                    const TC c2 = (u1r * rz + u1s * sz + u1t * tz) - (u3r * rx + u3s * sx + u3t * tx);
+                    const TC c3 = (u2r * rx + u2s * sx + u2t * tx) - (u1r * ry + u1s * sy + u1t * ty);
+                    const double sg_ = fld == 0 ? 1.0 : -1.0;
+                    rhs[3 * fld + 0] = sg_ * static_cast<double>(c1);
+                    rhs[3 * fld + 1] = sg_ * static_cast<double>(c2);
+                    rhs[3 * fld + 2] = sg_ * static_cast<double>(c3);
+                }
+            }
+            add_lifts<N, 6>(Fl, 0, i, j, k, rhs);
+            // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const double kn = A * kold[c] + DT * rhs[c];
+                __stcs(P.k + c * S + g, kn);
+                __stcs(P.u_out + c * S + g, Uf[c * CS + ms] + B * kn);
+            }
+        }
+    }
+}
+
+template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD>
+__global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const StageParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using L = Layout2<N, F32, EPB, PIPE, PAD>;
+    constexpr int NT = EPB * KS * N * N;
+    const int tid = threadIdx.x;
+    const int ntiles = (P.nelt + EPB - 1) / EPB;
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    double* sD = reinterpret_cast<double*>(smem + L::D);
+    double* sflux = reinterpret_cast<double*>(smem + L::flux);
+    for (int x = tid; x < N * N; x += NT) cp_async8(sD + x, P.D + x);
+    auto su = [&](int b) { return reinterpret_cast<double*>(smem + L::u0 + b * L::tile); };
+    auto sg = [&](int b) { return reinterpret_cast<ElemGeo*>(smem + L::geo0 + b * L::geo_b); };
+    auto sc = [&](int b) { return reinterpret_cast<int*>(smem + L::conn0 + b * L::conn_b); };
+    issue2<N, GEO, EPB, NT, PAD>(P, t * EPB, su(0), sg(0), sc(0), tid);
+    cp_async_commit();
+    if constexpr (!PIPE) {
+        cp_async_wait<0>();
+        __syncthreads();
+        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD>(P, t * EPB, su(0), sg(0), sc(0), sD, sflux,
+                                                   smem + L::uc, tid);
+    } else {
+        for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
+            const int b = n & 1;
+            cp_async_wait<0>();
+            __syncthreads();  // tile t resident; every thread is done with the other buffer
+            const int tn = t + gridDim.x;
+            if (tn < ntiles) issue2<N, GEO, EPB, NT, PAD>(P, tn * EPB, su(b ^ 1), sg(b ^ 1), sc(b ^ 1), tid);
+            cp_async_commit();
+            compute2<N, GEO, F32, KS, EPB, SPLIT, PAD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
+                                                       smem + L::uc, tid);
+        }
+        cp_async_wait<0>();
+    }
+}
+
+// Launch of one variant of the family.  PIPE: as many blocks as fit on the device
+// at once (queried with the occupancy calculator on the first call, which the
+// solver makes at creation, outside any stream capture), never more than tiles.
+template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD>
+cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
+    constexpr int threads = EPB * KS * N * N;
+    constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
+    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD>;
+    if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
+    static int resident = 0;
+    if (resident == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0, occ = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+        if (e != cudaSuccess) return e;
+        if (occ < 1) return cudaErrorInvalidConfiguration;
+        resident = occ * sms;
+    }
+    if (!p) return cudaSuccess;
+    const int tiles = (p->nelt + EPB - 1) / EPB;
+    const int blocks = PIPE ? (tiles < resident ? tiles : resident) : tiles;
+    kern<<<blocks, threads, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+}  // namespace stage
+}  // namespace nwb

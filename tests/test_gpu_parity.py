@@ -242,3 +242,26 @@ def test_every_launch_shape_matches_oracle(gpu, N, prec):
     assert 0 <= best < nv and len(ms) == nv and all(t > 0 for t in ms)
     np.testing.assert_array_equal(s.downloadState(), u)  # autotuning leaves the state alone
     s.finalize()
+
+
+@pytest.mark.parametrize("N,nel", [(4, (24, 24, 24)), (5, (20, 16, 16)), (6, (16, 16, 16)),
+                                   (7, (12, 12, 12)), (8, (16, 16, 12)), (9, (12, 12, 10))])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_every_launch_shape_on_meshes_of_many_tiles(gpu, N, nel, prec):
+    """Meshes of about a million nodes: several tiles per resident block, so the
+    persistent double-buffered shapes walk their whole tile loop (buffer swaps,
+    ragged last tile, neighbours in tiles that are in flight)."""
+    m = O.box_mesh(N, nel, (0, 0, 0), (1, 1.5, 1), (True, False, False))
+    s = solver_for(m, 1.0, prec)
+    u = random_state(m, 11)
+    want = O.rhs(m, 1.0, u)
+    dt = 0.5 * O.dxmin(m)
+    want_steps, _ = O.step(m, 1.0, dt, 2, u)
+    tol = RHS_TOL if prec == "fp64" else 1e-4
+    for v in range(s.info()["variant_count"]):
+        s.setVariant(v)
+        s.uploadState(u)
+        assert rel_max(s.evalRhs(), want) < tol, v
+        s.steps(dt, 2)
+        assert rel_l2(s.downloadState(), want_steps) < (STEP_TOL if prec == "fp64" else 1e-5), v
+    s.finalize()
