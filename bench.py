@@ -68,7 +68,7 @@ L2_BYTES = 126 * 1024 * 1024
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--steps", type=int, default=500)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["nwb", "reference"], default="nwb")
     p.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")

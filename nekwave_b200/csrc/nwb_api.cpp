@@ -210,6 +210,7 @@ struct nwb_solver {
     double* k = nullptr;
     int cur = 0;
     double* dD = nullptr;
+    double hD[100] = {};
     nwb::ElemGeo* dgeo = nullptr;
     int* dconn = nullptr;
     double* djac_e = nullptr;
@@ -252,6 +253,7 @@ struct nwb_solver {
         P.a = kRK4A[stage];
         P.b = kRK4B[stage];
         P.dt = dt;
+        for (int x = 0; x < N * N; ++x) P.Dc[x] = hD[x];
         return P;
     }
 
@@ -458,6 +460,7 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
     do { ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
          if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
     NWB_H2D(s->dD, D, sizeof(double) * N2);
+    for (int x = 0; x < N2; ++x) s->hD[x] = D[x];
     NWB_H2D(s->dw3, w3, sizeof(double) * N3);
     if (s->geo != nwb::GEO_NODAL) {
         NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(nelt), &tot));

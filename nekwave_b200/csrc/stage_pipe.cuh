@@ -19,6 +19,9 @@
 //   PAD    rows of the shared-memory tile are N+1 doubles apart (node (i,j,k) of
 //          an element at i + (N+1)(j + N k)), which spreads the traces of the
 //          r-faces (i = 0, N-1) and the rows of the r-derivative over the banks.
+//   CONSTD (with SPLIT, FP64) the plane loop is unrolled, so the t-derivative's
+//          D(k,l) are compile-time indices into the kernel's parameter copy of D
+//          and enter the FMAs as constant-bank operands instead of shared loads.
 //
 // In every form the face phase requests the neighbour values of all of a thread's
 // face points before it forms any flux, and each node's k is read before the
@@ -148,7 +151,7 @@ __device__ __forceinline__ void add_lifts(const double* Fl, int c0, int i, int j
 // Face phase and column phase of one tile whose u_in, geometry and connections
 // are resident in (su, sg, sc).  All threads of the block call it; threads
 // tid >= EPB*KS*N*N take part in the barrier only.
-template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD>
+template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid) {
@@ -163,6 +166,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     constexpr int CS = EPB * EN3;
     constexpr int FPT = (6 * N2 + TPE - 1) / TPE;    // face points per thread
     static_assert(!SPLIT || KS == 2, "the field split needs two threads per column");
+    static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
 
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
@@ -313,7 +317,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
         for (int c = 0; c < NC; ++c)
 #pragma unroll
             for (int l = 0; l < N; ++l) col[c][l] = V[c * CS + i + RP * j + PP * l];
-#pragma unroll 1
+#pragma unroll (CONSTD ? N : 1)
         for (int k = 0; k < N; ++k) {
             const int mn = i + N * j + N2 * k;           // node in natural numbering
             const int ms = i + RP * j + PP * k;          // node in shared memory
@@ -327,7 +331,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TC dr = Dr[l], ds = Ds[l];
-                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const TC dt = CONSTD ? static_cast<TC>(P.Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
                     Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
@@ -343,7 +347,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TC dr = Dr[l], ds = Ds[l];
-                    const TC dt = static_cast<TC>(sD[k + l * N]);
+                    const TC dt = CONSTD ? static_cast<TC>(P.Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
 #pragma unroll
@@ -474,7 +478,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     }
 }
 
-template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD>
+template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
+          bool CONSTD>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L = Layout2<N, F32, EPB, PIPE, PAD>;
@@ -494,7 +499,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
     if constexpr (!PIPE) {
         cp_async_wait<0>();
         __syncthreads();
-        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD>(P, t * EPB, su(0), sg(0), sc(0), sD, sflux,
+        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(0), sg(0), sc(0), sD, sflux,
                                                    smem + L::uc, tid);
     } else {
         for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
@@ -504,7 +509,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
             const int tn = t + gridDim.x;
             if (tn < ntiles) issue2<N, GEO, EPB, NT, PAD>(P, tn * EPB, su(b ^ 1), sg(b ^ 1), sc(b ^ 1), tid);
             cp_async_commit();
-            compute2<N, GEO, F32, KS, EPB, SPLIT, PAD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
+            compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
                                                        smem + L::uc, tid);
         }
         cp_async_wait<0>();
@@ -514,11 +519,12 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
 // Launch of one variant of the family.  PIPE: as many blocks as fit on the device
 // at once (queried with the occupancy calculator on the first call, which the
 // solver makes at creation, outside any stream capture), never more than tiles.
-template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD>
+template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
+          bool CONSTD>
 cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int threads = EPB * KS * N * N;
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
-    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD>;
+    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
     static int resident = 0;
     if (resident == 0) {
