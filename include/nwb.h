@@ -156,6 +156,11 @@ typedef struct nwb_solver_info {
     int minb;                     /* resident blocks the launch shape asks for     */
     int variant;                  /* current launch shape                          */
     int variant_count;            /* launch shapes available for this mesh         */
+    int structured[3];            /* elements per axis when the connections are those
+                                     of a structured box (x fastest, faces meeting
+                                     without rotation; neighbours then follow from
+                                     the element index), else 0                     */
+    int periodic_mask;            /* structured box: periodic axes, bit 0 x .. 2 z  */
 } nwb_solver_info;
 nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info);
 /* Energy of a device-resident state without allocating device memory.

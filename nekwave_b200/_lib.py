@@ -49,7 +49,8 @@ class SolverInfo(C.Structure):
                 ("stride", C.c_longlong), ("geometry", C.c_int), ("precision", C.c_int),
                 ("ks", C.c_int), ("epb", C.c_int), ("threads_per_block", C.c_int),
                 ("smem_bytes", C.c_int), ("device_bytes", C.c_longlong), ("ksmem", C.c_int),
-                ("minb", C.c_int), ("variant", C.c_int), ("variant_count", C.c_int)]
+                ("minb", C.c_int), ("variant", C.c_int), ("variant_count", C.c_int),
+                ("structured", C.c_int * 3), ("periodic_mask", C.c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/nwb.h declares.

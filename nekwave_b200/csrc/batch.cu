@@ -59,9 +59,10 @@ __device__ __forceinline__ void tile2(const StageParams& P, int e0, unsigned cha
     stage::cp_async_commit();
     stage::cp_async_wait<0>();
     __syncthreads();
+    stage::FaceGather<stage::face_points_per_thread<N, KS>()> G;
     stage::compute2<N, GEO_BOX, F32, KS, EPB, SPLIT, PAD>(P, e0, su, sg, sc, sD,
                                                           reinterpret_cast<double*>(smem + L2::flux),
-                                                          smem + L2::uc, tid);
+                                                          smem + L2::uc, tid, G);
 }
 
 template <int N, bool F32>
@@ -118,6 +119,8 @@ batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict
         P.flift = nullptr;
         P.fplus = nullptr;
         P.nfp = 0;
+        P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
+        P.spmask = 0;
         P.c0 = S.c0;
         P.a = dry ? 0.0 : c_rk4a[stage];
         P.b = dry ? 0.0 : c_rk4b[stage];
@@ -155,6 +158,8 @@ __device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, 
     P.flift = nullptr;
     P.fplus = nullptr;
     P.nfp = 0;
+    P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
+    P.spmask = 0;
     P.c0 = S.c0;
     P.a = dry ? 0.0 : c_rk4a[stage];
     P.b = dry ? 0.0 : c_rk4b[stage];

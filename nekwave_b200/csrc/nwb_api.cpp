@@ -211,6 +211,8 @@ struct nwb_solver {
     int cur = 0;
     double* dD = nullptr;
     double hD[100] = {};
+    int snel[3] = {0, 0, 0};  // structured box mesh (x-fastest elements), 0 = not
+    int spmask = 0;
     nwb::ElemGeo* dgeo = nullptr;
     int* dconn = nullptr;
     double* djac_e = nullptr;
@@ -254,6 +256,8 @@ struct nwb_solver {
         P.b = kRK4B[stage];
         P.dt = dt;
         for (int x = 0; x < N * N; ++x) P.Dc[x] = hD[x];
+        for (int d = 0; d < 3; ++d) P.snel[d] = snel[d];
+        P.spmask = spmask;
         return P;
     }
 
@@ -408,6 +412,64 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
 
 namespace {
 
+// Connection code of face f of element (ex,ey,ez) of a structured box mesh with
+// x-fastest element order (the order of the reference's createBoxMesh).
+int box_conn(int ex, int ey, int ez, int f, const int nel[3], int pm) {
+    const int nx = nel[0], ny = nel[1], nz = nel[2];
+    auto id = [&](int a, int b, int c) { return a + nx * (b + ny * c); };
+    int nb = -1;
+    switch (f) {
+        case 0: nb = ey > 0 ? id(ex, ey - 1, ez) : ((pm & 2) ? id(ex, ny - 1, ez) : -1); break;
+        case 1: nb = ex < nx - 1 ? id(ex + 1, ey, ez) : ((pm & 1) ? id(0, ey, ez) : -1); break;
+        case 2: nb = ey < ny - 1 ? id(ex, ey + 1, ez) : ((pm & 2) ? id(ex, 0, ez) : -1); break;
+        case 3: nb = ex > 0 ? id(ex - 1, ey, ez) : ((pm & 1) ? id(nx - 1, ey, ez) : -1); break;
+        case 4: nb = ez > 0 ? id(ex, ey, ez - 1) : ((pm & 4) ? id(ex, ey, nz - 1) : -1); break;
+        default: nb = ez < nz - 1 ? id(ex, ey, ez + 1) : ((pm & 4) ? id(ex, ey, 0) : -1); break;
+    }
+    static const int opp[6] = {2, 3, 0, 1, 5, 4};
+    return nb < 0 ? nwb::kConnPEC : ((nb << 6) | (opp[f] << 3));
+}
+
+// Recognises the connection table of a structured box mesh (elements x-fastest,
+// identity face orientations): the stage kernels can then find neighbours from
+// the element index.  Returns false and leaves nel at 0 for any other table.
+bool detect_structure(const std::vector<int>& conn, int nelt, int nel[3], int* pm) {
+    nel[0] = nel[1] = nel[2] = 0;
+    *pm = 0;
+    auto step = [&](int e, int f) { const int cd = conn[6 * static_cast<size_t>(e) + f];
+                                    return cd == nwb::kConnPEC ? -1 : (cd >> 6); };
+    int n[2] = {1, 1}, mask = 0;
+    const int face[2] = {1, 2};
+    for (int d = 0; d < 2; ++d) {
+        const int stride = d == 0 ? 1 : n[0];
+        int e = 0;
+        for (;;) {
+            const int nb = step(e, face[d]);
+            if (nb < 0) break;
+            if (nb == 0) { mask |= 1 << d; break; }
+            if (nb != e + stride || n[d] >= nelt) return false;
+            e = nb;
+            ++n[d];
+        }
+    }
+    if (nelt % (n[0] * n[1]) != 0) return false;
+    const int nz = nelt / (n[0] * n[1]);
+    const int zb = step(0, 4);
+    if (zb >= 0) {
+        if (zb != (nz - 1) * n[0] * n[1]) return false;
+        mask |= 4;
+    }
+    const int dims[3] = {n[0], n[1], nz};
+    for (int e = 0; e < nelt; ++e) {
+        const int ex = e % dims[0], ey = (e / dims[0]) % dims[1], ez = e / (dims[0] * dims[1]);
+        for (int f = 0; f < 6; ++f)
+            if (conn[6 * static_cast<size_t>(e) + f] != box_conn(ex, ey, ez, f, dims, mask)) return false;
+    }
+    for (int d = 0; d < 3; ++d) nel[d] = dims[d];
+    *pm = mask;
+    return true;
+}
+
 // Allocates and uploads a solver from analysed geometry.  m supplies the
 // per-node arrays of the general class and may be null for the affine classes.
 nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* D, const double* w3,
@@ -469,6 +531,7 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
         NWB_H2D(s->dgeo, A.egeo.data(), sizeof(nwb::ElemGeo) * nelt);
         NWB_H2D(s->dconn, A.conn.data(), sizeof(int) * 6 * static_cast<size_t>(nelt));
         NWB_H2D(s->djac_e, A.jac_e.data(), sizeof(double) * nelt);
+        detect_structure(A.conn, nelt, s->snel, &s->spmask);
     } else {
         const size_t nfp = static_cast<size_t>(s->nfp);
         try {
@@ -664,6 +727,8 @@ nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info) {
     info->variant = s->variant;
     info->variant_count = nwb::stage_variant_count(s->N, s->geo, s->f32);
     info->device_bytes = static_cast<long long>(s->device_bytes);
+    for (int d = 0; d < 3; ++d) info->structured[d] = s->snel[d];
+    info->periodic_mask = s->spmask;
     return NWB_OK;
 }
 

@@ -51,6 +51,8 @@ struct StageParams {
     long long nfp;
     double c0;              // flux penalty: 0 central, 1 upwind
     double a, b, dt;        // LSRK45 stage coefficients and step
+    int snel[3];            // structured box mesh: elements per axis (x fastest), or 0
+    int spmask;             // structured box mesh: periodic axes (bit 0 x, 1 y, 2 z)
     double Dc[100];         // D again, by value: kernels that index it with constants
                             // read it as an operand from the parameter bank
 };

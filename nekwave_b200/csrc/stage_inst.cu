@@ -45,13 +45,13 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (v.alg >= 2) {
-                static_assert(v.ksm == 0 && v.alg <= 17, "second family: k from L2, flags 0..15");
+                static_assert(v.ksm == 0 && v.alg <= 33, "second family: k from L2, flags 0..31");
                 constexpr int fl = v.alg - 2;
                 // the constant-bank D is an FP64 form; FP32-bulk runs the same shape without it
                 constexpr bool cd = (fl & 8) != 0 && !F32;
                 if constexpr (GEO == GEO_BOX || I == 0)
                     return launch2<NWB_N, GEO, F32, v.ks, v.epb, v.minb, (fl & 1) != 0, (fl & 2) != 0,
-                                   (fl & 4) != 0, cd>(p, st, cfg);
+                                   (fl & 4) != 0, cd, (fl & 16) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == 0) {

@@ -22,6 +22,11 @@
 //   CONSTD (with SPLIT, FP64) the plane loop is unrolled, so the t-derivative's
 //          D(k,l) are compile-time indices into the kernel's parameter copy of D
 //          and enter the FMAs as constant-bank operands instead of shared loads.
+//   EARLY  (without PIPE) the neighbour traces of the tile's face points are
+//          requested from global memory right after the tile's copies are issued,
+//          before the block waits for them, so both latencies overlap.  On a
+//          structured box mesh (StageParams::snel) the neighbour element follows
+//          from the element index, so no connection-table read precedes them.
 //
 // In every form the face phase requests the neighbour values of all of a thread's
 // face points before it forms any flux, and each node's k is read before the
@@ -148,13 +153,120 @@ __device__ __forceinline__ void add_lifts(const double* Fl, int c0, int i, int j
     }
 }
 
+// Neighbour element across face f of element e of a structured box mesh
+// (x-fastest element order, faces 0..5 = y-, x+, y+, x-, z-, z+), -1 where the
+// face lies on a non-periodic wall; the matching face is the opposite one with
+// the identity orientation.
+__device__ __forceinline__ int struct_neighbour(const StageParams& P, int ex, int ey, int ez, int e,
+                                                int f) {
+    const int nx = P.snel[0], ny = P.snel[1], nz = P.snel[2], pm = P.spmask;
+    const int sx = 1, sy = nx, sz = nx * ny;
+    switch (f) {
+        case 0: return ey > 0 ? e - sy : ((pm & 2) ? e + sy * (ny - 1) : -1);
+        case 1: return ex < nx - 1 ? e + sx : ((pm & 1) ? e - sx * (nx - 1) : -1);
+        case 2: return ey < ny - 1 ? e + sy : ((pm & 2) ? e - sy * (ny - 1) : -1);
+        case 3: return ex > 0 ? e - sx : ((pm & 1) ? e + sx * (nx - 1) : -1);
+        case 4: return ez > 0 ? e - sz : ((pm & 4) ? e + sz * (nz - 1) : -1);
+        default: return ez < nz - 1 ? e + sz : ((pm & 4) ? e - sz * (nz - 1) : -1);
+    }
+}
+
+// Neighbour values of the face points of one thread (FPT of them): the global
+// node vB across each point (-1: mirror) and its six field values.
+template <int FPT>
+struct FaceGather {
+    double nb[FPT][6];
+    long long vB[FPT];
+};
+
+// Fill a FaceGather.  FROM_SMEM: the tile is resident (connections from sc,
+// neighbours inside the tile from su); otherwise only global memory is read, so
+// it may run while the tile's copies are still in flight.
+template <int N, int GEO, int KS, int EPB, bool PAD, bool FROM_SMEM, int FPT>
+__device__ __forceinline__ void gather2(const StageParams& P, const int e0, const double* su,
+                                        const int* sc, const int tid, FaceGather<FPT>& G) {
+    constexpr int N2 = N * N, N3 = N2 * N;
+    constexpr int TPE = KS * N2;
+    constexpr int CS = EPB * (PAD ? N2 * (N + 1) : N3);
+    const int team = tid / TPE;
+    const int lt = tid - team * TPE;
+    const int nvalid = min(EPB, P.nelt - e0);
+    const int e = e0 + team;
+    const long long S = P.stride;
+    // the tile-resident form reads the connection table from shared memory; the
+    // early form uses the structure when there is one
+    const bool structured = !FROM_SMEM && P.snel[0] > 0;
+    int ex = 0, ey = 0, ez = 0;
+    if (structured) {
+        ex = e % P.snel[0];
+        const int r = e / P.snel[0];
+        ey = r % P.snel[1];
+        ez = r / P.snel[1];
+    }
+#pragma unroll
+    for (int q = 0; q < FPT; ++q) {
+        const int fp = lt + q * TPE;
+        long long vB = -1;
+        if (team < nvalid && fp < 6 * N2) {
+            const int f = fp / N2;
+            const int pq = fp - f * N2;
+            const int p = pq % N, qq = pq / N;
+            int eB = -1;
+            if constexpr (GEO == GEO_NODAL) {
+                vB = P.fplus[(static_cast<long long>(e) * 6 + f) * N2 + pq];
+                if (vB >= 0) eB = static_cast<int>(vB / N3);
+            } else if (structured) {
+                eB = struct_neighbour(P, ex, ey, ez, e, f);
+                if (eB >= 0) {
+                    constexpr int opp[6] = {2, 3, 0, 1, 5, 4};
+                    vB = static_cast<long long>(eB) * N3 + face_local<N>(opp[f], p, qq);
+                }
+            } else {
+                int cd;
+                if constexpr (FROM_SMEM) cd = sc[team * 6 + f];
+                else cd = __ldg(P.conn + e * 6 + f);
+                if (cd != kConnPEC) {
+                    const int fB = (cd >> 3) & 7, o = cd & 7;
+                    eB = cd >> 6;
+                    int a = (o & 4) ? qq : p;
+                    int b = (o & 4) ? p : qq;
+                    if (o & 1) a = N - 1 - a;
+                    if (o & 2) b = N - 1 - b;
+                    vB = static_cast<long long>(eB) * N3 + face_local<N>(fB, a, b);
+                }
+            }
+            if (vB >= 0) {
+                bool in_tile = false;
+                if constexpr (FROM_SMEM) in_tile = eB >= e0 && eB < e0 + nvalid;
+                if (in_tile) {
+                    const int el = eB - e0;
+                    const int sidx = el * (CS / EPB) + pidx<N, PAD>(static_cast<int>(vB - static_cast<long long>(eB) * N3));
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) G.nb[q][c] = su[c * CS + sidx];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) G.nb[q][c] = __ldg(P.u_in + c * S + vB);
+                }
+            }
+        }
+        G.vB[q] = vB;
+    }
+}
+
 // Face phase and column phase of one tile whose u_in, geometry and connections
 // are resident in (su, sg, sc).  All threads of the block call it; threads
 // tid >= EPB*KS*N*N take part in the barrier only.
-template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false>
+template <int N, int KS>
+__host__ __device__ constexpr int face_points_per_thread() {
+    return (6 * N * N + KS * N * N - 1) / (KS * N * N);
+}
+
+template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
+          bool EARLY = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
-                                         double* sflux, unsigned char* smem_uc, const int tid) {
+                                         double* sflux, unsigned char* smem_uc, const int tid,
+                                         FaceGather<face_points_per_thread<N, KS>()>& G) {
     using TC = typename std::conditional<F32, float, double>::type;
     constexpr int N2 = N * N, N3 = N2 * N;
     constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
@@ -200,46 +312,9 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 
     // ---- face phase: neighbour values of all of this thread's face points are
     // requested first, then the fluxes are formed
+    if constexpr (!EARLY) gather2<N, GEO, KS, EPB, PAD, true>(P, e0, su, sc, tid, G);
     if (active) {
         const double* U = su + team * EN3;
-        double nb[FPT][6];
-        long long vBs[FPT];
-#pragma unroll
-        for (int q = 0; q < FPT; ++q) {
-            const int fp = lt + q * TPE;
-            long long vB = -1;
-            if (fp < 6 * N2) {
-                const int f = fp / N2;
-                const int pq = fp - f * N2;
-                const int p = pq % N, qq = pq / N;
-                if constexpr (GEO == GEO_NODAL) {
-                    vB = P.fplus[(static_cast<long long>(e) * 6 + f) * N2 + pq];
-                } else {
-                    const int cd = sc[team * 6 + f];
-                    if (cd != kConnPEC) {
-                        const int eB = cd >> 6, fB = (cd >> 3) & 7, o = cd & 7;
-                        int a = (o & 4) ? qq : p;
-                        int b = (o & 4) ? p : qq;
-                        if (o & 1) a = N - 1 - a;
-                        if (o & 2) b = N - 1 - b;
-                        vB = static_cast<long long>(eB) * N3 + face_local<N>(fB, a, b);
-                    }
-                }
-                if (vB >= 0) {
-                    const long long eB = vB / N3;
-                    if (eB >= e0 && eB < e0 + nvalid) {
-                        const int el = static_cast<int>(eB - e0);
-                        const int sidx = el * EN3 + pidx<N, PAD>(static_cast<int>(vB - eB * N3));
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) nb[q][c] = su[c * CS + sidx];
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < 6; ++c) nb[q][c] = __ldg(P.u_in + c * S + vB);
-                    }
-                }
-            }
-            vBs[q] = vB;
-        }
 #pragma unroll
         for (int q = 0; q < FPT; ++q) {
             const int fp = lt + q * TPE;
@@ -265,13 +340,13 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 lift = G.lift[f];
             }
             double jmp[6];
-            if (vBs[q] < 0) {
+            if (G.vB[q] < 0) {
                 // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
                 jmp[0] = -2.0 * Exm; jmp[1] = -2.0 * Eym; jmp[2] = -2.0 * Ezm;
                 jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
             } else {
-                jmp[0] = nb[q][0] - Exm; jmp[1] = nb[q][1] - Eym; jmp[2] = nb[q][2] - Ezm;
-                jmp[3] = nb[q][3] - Hxm; jmp[4] = nb[q][4] - Hym; jmp[5] = nb[q][5] - Hzm;
+                jmp[0] = G.nb[q][0] - Exm; jmp[1] = G.nb[q][1] - Eym; jmp[2] = G.nb[q][2] - Ezm;
+                jmp[3] = G.nb[q][3] - Hxm; jmp[4] = G.nb[q][4] - Hym; jmp[5] = G.nb[q][5] - Hzm;
             }
             TC fl[6];
             numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
@@ -479,7 +554,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 }
 
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD>
+          bool CONSTD, bool EARLY>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L = Layout2<N, F32, EPB, PIPE, PAD>;
@@ -494,13 +569,16 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
     auto su = [&](int b) { return reinterpret_cast<double*>(smem + L::u0 + b * L::tile); };
     auto sg = [&](int b) { return reinterpret_cast<ElemGeo*>(smem + L::geo0 + b * L::geo_b); };
     auto sc = [&](int b) { return reinterpret_cast<int*>(smem + L::conn0 + b * L::conn_b); };
+    static_assert(!(EARLY && PIPE), "the early gather belongs to the one-tile form");
+    FaceGather<face_points_per_thread<N, KS>()> G;
     issue2<N, GEO, EPB, NT, PAD>(P, t * EPB, su(0), sg(0), sc(0), tid);
     cp_async_commit();
     if constexpr (!PIPE) {
+        if constexpr (EARLY) gather2<N, GEO, KS, EPB, PAD, false>(P, t * EPB, nullptr, nullptr, tid, G);
         cp_async_wait<0>();
         __syncthreads();
-        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(0), sg(0), sc(0), sD, sflux,
-                                                   smem + L::uc, tid);
+        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY>(P, t * EPB, su(0), sg(0), sc(0), sD,
+                                                                  sflux, smem + L::uc, tid, G);
     } else {
         for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
             const int b = n & 1;
@@ -510,7 +588,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
             if (tn < ntiles) issue2<N, GEO, EPB, NT, PAD>(P, tn * EPB, su(b ^ 1), sg(b ^ 1), sc(b ^ 1), tid);
             cp_async_commit();
             compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
-                                                       smem + L::uc, tid);
+                                                               smem + L::uc, tid, G);
         }
         cp_async_wait<0>();
     }
@@ -520,11 +598,11 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
 // at once (queried with the occupancy calculator on the first call, which the
 // solver makes at creation, outside any stream capture), never more than tiles.
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD>
+          bool CONSTD, bool EARLY>
 cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int threads = EPB * KS * N * N;
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
-    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD>;
+    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
     static int resident = 0;
     if (resident == 0) {

@@ -125,7 +125,9 @@ class DgSolver:
         h = self._need()
         i = SolverInfo()
         check(_lib.lib().nwb_solver_get_info(h, C.byref(i)))
-        return {k: getattr(i, k) for k, _ in SolverInfo._fields_}
+        out = {k: getattr(i, k) for k, _ in SolverInfo._fields_}
+        out["structured"] = tuple(i.structured)
+        return out
 
     def launchCount(self) -> int:
         n = C.c_longlong()

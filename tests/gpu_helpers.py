@@ -40,3 +40,30 @@ def smooth_state(m, seed):
         u[c * m.npts:(c + 1) * m.npts] = np.exp(-((m.x - r0[0]) ** 2 + (m.y - r0[1]) ** 2 +
                                                   (m.zc - r0[2]) ** 2) / sig ** 2)
     return u
+
+
+def shuffled_box_mesh(N, nel, lo, hi, seed, rotate=True):
+    """A box mesh (PEC walls) whose elements are numbered in a seeded random order
+    and, with rotate, every other element has its local frame turned 90 degrees
+    about z (its faces renumbered accordingly): neighbour faces then meet with
+    non-identity orientations and the element order carries no structure."""
+    corners, fk, fb, ff = O.box_corners(nel, lo, hi, (False, False, False))
+    nelt = corners.shape[0]
+    rot = (np.arange(nelt) % 2 == 1) if rotate else np.zeros(nelt, bool)
+    newface = np.array([3, 0, 1, 2, 4, 5])  # old face -> face of the turned frame
+    cr, fk2, fb2, ff2 = corners.copy(), fk.copy(), fb.copy(), ff.copy()
+    for e in np.nonzero(rot)[0]:
+        cr[e] = corners[e][[1, 2, 3, 0, 5, 6, 7, 4]]
+        fk2[e, newface] = fk[e]
+        fb2[e, newface] = fb[e]
+        ff2[e, newface] = ff[e]
+    has = fb2 >= 0
+    nbrot = np.zeros_like(has)
+    nbrot[has] = rot[fb2[has]]
+    ff2[nbrot] = newface[ff2[nbrot]]
+    perm = np.random.Generator(np.random.PCG64(seed)).permutation(nelt)
+    inv = np.empty(nelt, np.int64)
+    inv[perm] = np.arange(nelt)
+    fb3 = fb2[perm].copy()
+    fb3[fb3 >= 0] = inv[fb3[fb3 >= 0]]
+    return O.hex_mesh(N, cr[perm], fk2[perm], fb3, ff2[perm])

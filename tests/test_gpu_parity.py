@@ -13,6 +13,7 @@ import os
 import numpy as np
 import pytest
 
+from nekwave_b200 import DgSolver
 from oracle import oracle as O
 from tests.gpu_helpers import random_state, rel_l2, rel_max, smooth_state, solver_for
 
@@ -265,3 +266,42 @@ def test_every_launch_shape_on_meshes_of_many_tiles(gpu, N, nel, prec):
         s.steps(dt, 2)
         assert rel_l2(s.downloadState(), want_steps) < (STEP_TOL if prec == "fp64" else 1e-5), v
     s.finalize()
+
+
+@pytest.mark.parametrize("N", [3, 5, 6, 8])
+@pytest.mark.parametrize("rotate", [False, True])
+def test_shuffled_and_rotated_elements(gpu, N, rotate):
+    """Element numbering without structure, and (rotate) faces that meet with
+    turned frames: the connection-table path of the face phase, with
+    non-identity orientations, for every launch shape of the geometry class."""
+    from tests.gpu_helpers import shuffled_box_mesh
+    m = shuffled_box_mesh(N, (3, 4, 2), (0, 0, 0), (1.5, 1, 0.75), 5, rotate)
+    s = solver_for(m, 1.0)
+    info = s.info()
+    assert info["structured"] == (0, 0, 0)
+    assert info["geometry"] == (1 if rotate else 0)
+    u = random_state(m, 4)
+    want = O.rhs(m, 1.0, u)
+    dt = 0.5 * O.dxmin(m)
+    want_steps, _ = O.step(m, 1.0, dt, 2, u)
+    for v in range(info["variant_count"]):
+        s.setVariant(v)
+        s.uploadState(u)
+        assert rel_max(s.evalRhs(), want) < RHS_TOL, v
+        s.steps(dt, 2)
+        assert rel_l2(s.downloadState(), want_steps) < STEP_TOL, v
+    s.finalize()
+
+
+@pytest.mark.parametrize("per", [(False, False, False), (True, False, True), (True, True, True)])
+def test_structured_box_is_recognised(gpu, per):
+    m = O.box_mesh(6, (4, 3, 2), (0, 0, 0), (1, 1, 1), per)
+    s = solver_for(m, 1.0)
+    info = s.info()
+    assert info["structured"] == (4, 3, 2)
+    assert info["periodic_mask"] == sum(1 << d for d in range(3) if per[d])
+    s.finalize()
+    b = DgSolver("fp64")
+    b.initializeBox(6, (4, 3, 2), (0, 0, 0), (1, 1, 1), 1.0, periodic=per)
+    assert b.info()["structured"] == (4, 3, 2)
+    b.finalize()
