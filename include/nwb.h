@@ -250,7 +250,7 @@ nwb_status nwb_pool_info(const nwb_pool* p, size_t* used_bytes, size_t* budget_b
 /* Stage launch mode: 0 = one persistent launch per stage for every N (tiles
  * handed out by an atomic counter, largest first), 1 = one launch per N present,
  * each with that N's tuned single-mesh launch shape, as parallel branches of the
- * step graph.  nwb_pool_autotune times both on the resident cavities (timing
+ * step graph (the default of a new pool).  nwb_pool_autotune times both on the resident cavities (timing
  * launches with a = b = dt = 0 leave every state as it is) and keeps the faster;
  * ms_out (optional) receives the two per-step stage times. */
 nwb_status nwb_pool_set_mode(nwb_pool* p, int mode);

@@ -123,7 +123,7 @@ struct nwb_pool {
     nwb::WorkItem* d_work_n = nullptr;
     int work_n_cap = 0;
     int n_off[11] = {}, n_cnt[11] = {};
-    int mode = 0;  // 0: one persistent launch for every N, 1: one launch per N
+    int mode = 1;  // 0: one persistent launch for every N, 1: one launch per N (default)
     cudaStream_t side[11] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[11] = {};
     cudaGraphExec_t graph = nullptr;

@@ -1,12 +1,21 @@
 """Continuous-batching server of cavity solves on one GPU.
 
 Requests (box cavity, order, final time, Gaussian pulse, 8 probes) arrive on a
-stream.  The server admits them into a CavityPool in arrival order as HBM budget
-and slots free up, keeps their fields resident, advances every admitted cavity
-together (one persistent launch per LSRK stage for all of them), and as each
-finishes returns its probe traces and energy history and frees its memory.
-Requests that arrive while others are on the GPU join the running batch at the
-next step boundary.  Latency = completion time - arrival time.
+stream.  The server admits them into a CavityPool as HBM budget and slots free up,
+keeps their fields resident, advances every admitted cavity together (one launch
+per N present per LSRK stage, all in one CUDA graph), and as each finishes returns
+its probe traces and energy history and frees its memory.  Requests that arrive
+while others are on the GPU join the running batch at the next step boundary.
+Latency = completion time - arrival time.
+
+Admission policy:
+  "fifo"  arrival order, as many as the budget holds (every admitted cavity
+          shares the GPU: processor sharing);
+  "sjf"   shortest remaining work first among the waiting requests, and new
+          admissions only while the resident cavities hold fewer than
+          ``saturation_nodes`` nodes -- enough to keep HBM busy, so admitting more
+          would only stretch every running request.  A request larger than that
+          runs on its own, as in the serial path; small ones batch together.
 
 The serial baseline serves the same stream one request at a time with the
 single-mesh FP64 solver (DgSolver), the reference's execution model.
@@ -14,7 +23,6 @@ single-mesh FP64 solver (DgSolver), the reference's execution model.
 from __future__ import annotations
 
 import time
-from collections import deque
 from dataclasses import dataclass
 
 import numpy as np
@@ -39,10 +47,15 @@ class Result:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 512, precision: str = "fp32",
-                 chunk: int = 4, energy_every: int = 10):
+                 chunk: int = 4, energy_every: int = 10, policy: str = "sjf",
+                 saturation_nodes: int = 8 << 20):
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy must be 'fifo' or 'sjf'")
         self.pool = CavityPool(hbm_budget_bytes, max_slots=max_slots, precision=precision)
         self.chunk = int(chunk)
         self.energy_every = int(energy_every)
+        self.policy = policy
+        self.saturation_nodes = int(saturation_nodes)
 
     def close(self):
         self.pool.close()
@@ -58,7 +71,7 @@ class Server:
         """Serve the stream in real time (arrivals replayed at time_scale x the
         request timestamps).  Returns the results in request order and the
         wall time of the whole run."""
-        pending = deque()
+        pending = []
         arrivals = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
         nxt = 0
         running = {}            # slot -> (request index, admit time)
@@ -70,14 +83,21 @@ class Server:
             while nxt < len(arrivals) and requests[arrivals[nxt]].arrival * time_scale <= t:
                 pending.append(arrivals[nxt])
                 nxt += 1
-            while pending:                       # FIFO admission by HBM budget
+            if self.policy == "sjf":
+                pending.sort(key=lambda i: requests[i].dof_stages)
+            resident = sum(requests[i].npts for i, _ in running.values())
+            while pending:
                 i = pending[0]
+                if (self.policy == "sjf" and running and
+                        resident + requests[i].npts > self.saturation_nodes):
+                    break
                 try:
                     s = self.admit(requests[i])
                 except PoolFull:
                     break
-                pending.popleft()
+                pending.pop(0)
                 running[s] = (i, now())
+                resident += requests[i].npts
             if not running:
                 if nxt < len(arrivals):          # idle until the next arrival
                     wait = requests[arrivals[nxt]].arrival * time_scale - now()

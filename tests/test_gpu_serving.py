@@ -15,9 +15,11 @@ def small_stream(n=8, rate=200.0):
     return serving_requests(n, rate, seed=5, max_nel=5, max_order=5)
 
 
-def test_each_request_same_alone_and_in_the_mix(gpu):
+@pytest.mark.parametrize("policy", ["fifo", "sjf"])
+def test_each_request_same_alone_and_in_the_mix(gpu, policy):
     reqs = small_stream()
-    srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=3, energy_every=1)
+    srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=3, energy_every=1, policy=policy,
+                 saturation_nodes=20000)
     mixed, wall = srv.run(reqs)
     srv.close()
     assert all(r is not None for r in mixed)
@@ -41,6 +43,20 @@ def test_requests_overlap_on_the_device(gpu):
     srv.close()
     spans = sorted((r.admitted, r.finished) for r in res)
     assert any(spans[k + 1][0] < spans[k][1] for k in range(len(spans) - 1))
+
+
+def test_sjf_admits_the_smallest_waiting_request_first(gpu):
+    """All requests waiting at once, residency capped below any two of them: they
+    run one at a time in order of work."""
+    reqs = small_stream(6, rate=1e9)
+    srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=2, policy="sjf", saturation_nodes=1)
+    res, _ = srv.run(reqs)
+    srv.close()
+    order = [r.request for r in sorted(res, key=lambda r: r.admitted)]
+    work = [reqs[i].dof_stages for i in order]
+    assert work == sorted(work)
+    spans = sorted((r.admitted, r.finished) for r in res)
+    assert all(spans[k + 1][0] >= spans[k][1] for k in range(len(spans) - 1))
 
 
 def test_serving_energy_matches_single_mesh_solver(gpu):
