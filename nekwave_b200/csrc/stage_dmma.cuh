@@ -1,0 +1,157 @@
+// stage_dmma.cuh -- fused LSRK45 stage for 8 points per direction, axis-aligned
+// elements, FP64, with the r and s contractions on the FP64 tensor cores
+// (mma.sync m8n8k4 f64) and the residual split by field between two warps.
+//
+// Why: in the SIMT forms every lane reads, for each r and s derivative it forms,
+// the N values of a row or column from shared memory, and a 64-bit warp load costs
+// two wavefronts however many lanes share an address; ncu shows those loads
+// keeping the L1/shared pipe at 80-90 % at N = 8.  As an 8x8x8 product per plane
+// and component, a warp reads each node value once per direction (one 64-bit
+// fragment load per lane per k-step) and keeps D in two registers.  tcgen05 has no
+// FP64 kind; mma.sync .f64 is sm_100a's FP64 tensor-core instruction.
+//
+// Block = one element, 64 threads = 2 warps:
+//   1. cp.async of u_in (16-byte copies), D, geometry, connections; k lines of the
+//      element into L2;
+//   2. face phase (face_phase2, one thread per face point, six per thread);
+//   3. warp 0 forms the E residual from V = H (+curl H), warp 1 the H residual from
+//      V = E (-curl E).  Lane 4g + t owns nodes (i = 2t, 2t+1; j = g) of every
+//      plane k.  Per plane: the r derivatives of Vz, Vy in the original form
+//      (A = rows of the plane, B = D^T) and the s derivatives of Vz, Vx in the
+//      swapped form (A = D, B = columns of the plane) land on the same two nodes;
+//      the t derivatives of Vy, Vx are SIMT sums over the lane's two node columns,
+//      read once into registers, with D(k,l) from the kernel's parameter bank.
+//      Then the lifted face terms in face order 0..5 and the LSRK update in FP64,
+//      two adjacent nodes per 16-byte access.
+// Fragment layout (m8n8k4, A row-major 8x4, B column-major 4x8, C 8x8): lane
+// L = 4g + t holds A[g][t], B[t][g], C[g][2t] and C[g][2t+1].
+#pragma once
+
+#include "stage_mma.cuh"
+#include "stage_pipe.cuh"
+
+namespace nwb {
+namespace stage {
+
+struct DmmaLayout8 {
+    static constexpr int u = 0;                                   // [6][512] doubles
+    static constexpr int geo = u + 6 * 512 * 8;
+    static constexpr int conn = geo + static_cast<int>(sizeof(ElemGeo));
+    static constexpr int D = conn + 32;
+    static constexpr int flux = D + 64 * 8;                       // [6 faces][6 comps][64]
+    static constexpr int total = flux + 36 * 64 * 8;
+};
+
+template <int MINB>
+__global__ void __launch_bounds__(64, MINB) stage_dmma8_kernel(const StageParams P) {
+    constexpr int N = 8, N3 = 512;
+    using L = DmmaLayout8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* su = reinterpret_cast<double*>(smem + L::u);
+    ElemGeo* sg = reinterpret_cast<ElemGeo*>(smem + L::geo);
+    int* sc = reinterpret_cast<int*>(smem + L::conn);
+    double* sD = reinterpret_cast<double*>(smem + L::D);
+    double* sflux = reinterpret_cast<double*>(smem + L::flux);
+    const int e = blockIdx.x;
+    const int tid = threadIdx.x;
+
+    issue2<N, GEO_BOX, 1, 64, false>(P, e, su, sg, sc, tid);
+    cp_async8(sD + tid, P.D + tid);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    FaceGather<face_points_per_thread<N, 1>()> G;
+    face_phase2<N, GEO_BOX, false, 1, 1, false, false>(P, e, su, sg, sc, sflux, tid, G);
+    __syncthreads();
+
+    const int warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int src = warp == 0 ? 3 : 0;   // differentiated field
+    const int dst = 3 - src;             // residual components formed
+    const double sgn = warp == 0 ? 1.0 : -1.0;
+    const double* V = su + src * N3;
+    const double d0 = sD[g + 8 * t];        // D(q = g, l = t)
+    const double d1 = sD[g + 8 * (4 + t)];  // D(q = g, l = 4 + t)
+    // the lane's two node columns of Vx and Vy (t derivatives)
+    double cx[8][2], cy[8][2];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const double2 a = *reinterpret_cast<const double2*>(V + 0 * N3 + 64 * l + 8 * g + 2 * t);
+        const double2 b = *reinterpret_cast<const double2*>(V + 1 * N3 + 64 * l + 8 * g + 2 * t);
+        cx[l][0] = a.x; cx[l][1] = a.y;
+        cy[l][0] = b.x; cy[l][1] = b.y;
+    }
+    const double rx = sg->met[0], sy = sg->met[4], tz = sg->met[8];
+    const double A = P.a, B = P.b, DT = P.dt;
+    const long long S = P.stride;
+    const long long ebase = static_cast<long long>(e) * N3;
+    const double* Fl = sflux;
+
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int ms = 64 * k + 8 * g + 2 * t;  // first of the lane's two nodes
+        double2 kold[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            kold[c] = __ldcg(reinterpret_cast<const double2*>(P.k + (dst + c) * S + ebase + ms));
+        // r (original form): A[g][t] = V(l = t, j = g, k)
+        double zr0 = 0.0, zr1 = 0.0, yr0 = 0.0, yr1 = 0.0;
+        dmma_f64(zr0, zr1, V[2 * N3 + 64 * k + 8 * g + t], d0);
+        dmma_f64(zr0, zr1, V[2 * N3 + 64 * k + 8 * g + 4 + t], d1);
+        dmma_f64(yr0, yr1, V[1 * N3 + 64 * k + 8 * g + t], d0);
+        dmma_f64(yr0, yr1, V[1 * N3 + 64 * k + 8 * g + 4 + t], d1);
+        // s (swapped form): B[t][g] = V(i = g, l = t, k)
+        double zs0 = 0.0, zs1 = 0.0, xs0 = 0.0, xs1 = 0.0;
+        dmma_f64(zs0, zs1, d0, V[2 * N3 + 64 * k + 8 * t + g]);
+        dmma_f64(zs0, zs1, d1, V[2 * N3 + 64 * k + 8 * (4 + t) + g]);
+        dmma_f64(xs0, xs1, d0, V[0 * N3 + 64 * k + 8 * t + g]);
+        dmma_f64(xs0, xs1, d1, V[0 * N3 + 64 * k + 8 * (4 + t) + g]);
+        // t: sums over the cached columns, D(k, l) from the parameter bank
+        double yt0 = 0.0, yt1 = 0.0, xt0 = 0.0, xt1 = 0.0;
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            const double dk = P.Dc[k + 8 * l];
+            yt0 += dk * cy[l][0]; yt1 += dk * cy[l][1];
+            xt0 += dk * cx[l][0]; xt1 += dk * cx[l][1];
+        }
+        double rhs0[3], rhs1[3];
+        rhs0[0] = sgn * (sy * zs0 - tz * yt0);
+        rhs0[1] = sgn * (tz * xt0 - rx * zr0);
+        rhs0[2] = sgn * (rx * yr0 - sy * xs0);
+        rhs1[0] = sgn * (sy * zs1 - tz * yt1);
+        rhs1[1] = sgn * (tz * xt1 - rx * zr1);
+        rhs1[2] = sgn * (rx * yr1 - sy * xs1);
+        add_lifts<N, 3>(Fl, dst, 2 * t, g, k, rhs0);
+        add_lifts<N, 3>(Fl, dst, 2 * t + 1, g, k, rhs1);
+        // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double kn0 = A * kold[c].x + DT * rhs0[c];
+            const double kn1 = A * kold[c].y + DT * rhs1[c];
+            const double2 uo = *reinterpret_cast<const double2*>(su + (dst + c) * N3 + ms);
+            __stcs(reinterpret_cast<double2*>(P.k + (dst + c) * S + ebase + ms), make_double2(kn0, kn1));
+            __stcs(reinterpret_cast<double2*>(P.u_out + (dst + c) * S + ebase + ms),
+                   make_double2(uo.x + B * kn0, uo.y + B * kn1));
+        }
+    }
+}
+
+template <int MINB>
+cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
+    constexpr int smem = DmmaLayout8::total;
+    auto kern = stage_dmma8_kernel<MINB>;
+    if (cfg) *cfg = StageConfig{1, 1, 64, smem, 0, MINB};
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (!p) return cudaSuccess;
+    kern<<<p->nelt, 64, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+}  // namespace stage
+}  // namespace nwb

@@ -3,6 +3,7 @@
 #include "stage_kernel.cuh"
 #include "stage_mma.cuh"
 #include "stage_pipe.cuh"
+#include "stage_dmma.cuh"
 #include "stage_variants.h"
 
 #ifndef NWB_N
@@ -28,10 +29,10 @@ constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
 constexpr int count_simt() {
     int n = 0;
-    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1;
+    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1 && kShapes[i].alg != 40;
     return n;
 }
-constexpr int kNumSimt = count_simt();  // every variant but the FP64 tensor-core ones (last)
+constexpr int kNumSimt = count_simt();  // every variant but the FP64-only tensor-core ones (last)
 
 // every variant for the axis-aligned class, variant 0 for the others
 template <int GEO, bool F32, int I>
@@ -44,7 +45,12 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                     return launch_mma8<v.minb>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
-            } else if constexpr (v.alg >= 2) {
+            } else if constexpr (v.alg == 40) {
+                if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
+                    return launch_dmma8<v.minb>(p, st, cfg);
+                else
+                    return cudaErrorInvalidValue;
+            } else if constexpr (v.alg >= 2 && v.alg <= 33) {
                 static_assert(v.ksm == 0 && v.alg <= 33, "second family: k from L2, flags 0..31");
                 constexpr int fl = v.alg - 2;
                 // the constant-bank D is an FP64 form; FP32-bulk runs the same shape without it

@@ -261,57 +261,27 @@ __host__ __device__ constexpr int face_points_per_thread() {
     return (6 * N * N + KS * N * N - 1) / (KS * N * N);
 }
 
-template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
-          bool EARLY = false>
-__device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
-                                         const ElemGeo* sg, const int* sc, const double* sD,
-                                         double* sflux, unsigned char* smem_uc, const int tid,
-                                         FaceGather<face_points_per_thread<N, KS>()>& G) {
+// Face phase of one tile: one thread per face point (FPT per thread), neighbour
+// values of all of a thread's points requested first (unless EARLY already did),
+// then the numerical flux of each point times its lift, stored in sflux
+// [team][face][component][point].  The caller synchronises afterwards.
+template <int N, int GEO, bool F32, int KS, int EPB, bool PAD, bool EARLY>
+__device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, const double* su,
+                                            const ElemGeo* sg, const int* sc, double* sflux,
+                                            const int tid,
+                                            FaceGather<face_points_per_thread<N, KS>()>& G) {
     using TC = typename std::conditional<F32, float, double>::type;
-    constexpr int N2 = N * N, N3 = N2 * N;
-    constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
-    constexpr int PP = RP * N;                       // plane pitch
-    constexpr int EN3 = PP * N;                      // element stride
+    constexpr int N2 = N * N;
+    constexpr int RP = PAD ? N + 1 : N;
+    constexpr int EN3 = RP * N * N;
     constexpr int TPE = KS * N2;
-    constexpr int NT = EPB * TPE;
-    constexpr int KPT = (N + KS - 1) / KS;
     constexpr int CS = EPB * EN3;
-    constexpr int FPT = (6 * N2 + TPE - 1) / TPE;    // face points per thread
-    static_assert(!SPLIT || KS == 2, "the field split needs two threads per column");
-    static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
-
+    constexpr int FPT = face_points_per_thread<N, KS>();
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
-    const int loc = lt % N2;
-    const int h = lt / N2;
-    const int i = loc % N;
-    const int j = loc / N;
     const int nvalid = min(EPB, P.nelt - e0);
     const int e = e0 + team;
     const bool active = team < nvalid;
-    const long long S = P.stride;
-
-    const TC* s_uc;
-    if constexpr (F32) {
-        // FP32 copy of the tile as deviations from the element's centre node: the
-        // derivatives are unchanged (rows of D sum to zero) and the rounding error
-        // scales with the variation across the element instead of |u|
-        TC* w = reinterpret_cast<TC*>(smem_uc);
-        constexpr int centre = (N / 2) * (1 + RP + PP);
-        const int cnt = tid < NT ? nvalid * EN3 : 0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-            for (int x = tid; x < cnt; x += NT) {
-                const double ref = su[c * CS + (x / EN3) * EN3 + centre];
-                w[c * CS + x] = static_cast<float>(su[c * CS + x] - ref);
-            }
-        s_uc = w;
-    } else {
-        s_uc = reinterpret_cast<const TC*>(su);
-    }
-
-    // ---- face phase: neighbour values of all of this thread's face points are
-    // requested first, then the fluxes are formed
     if constexpr (!EARLY) gather2<N, GEO, KS, EPB, PAD, true>(P, e0, su, sc, tid, G);
     if (active) {
         const double* U = su + team * EN3;
@@ -359,6 +329,58 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
             for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
         }
     }
+}
+
+template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
+          bool EARLY = false>
+__device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
+                                         const ElemGeo* sg, const int* sc, const double* sD,
+                                         double* sflux, unsigned char* smem_uc, const int tid,
+                                         FaceGather<face_points_per_thread<N, KS>()>& G) {
+    using TC = typename std::conditional<F32, float, double>::type;
+    constexpr int N2 = N * N, N3 = N2 * N;
+    constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
+    constexpr int PP = RP * N;                       // plane pitch
+    constexpr int EN3 = PP * N;                      // element stride
+    constexpr int TPE = KS * N2;
+    constexpr int NT = EPB * TPE;
+    constexpr int KPT = (N + KS - 1) / KS;
+    constexpr int CS = EPB * EN3;
+    static_assert(!SPLIT || KS == 2, "the field split needs two threads per column");
+    static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
+
+    const int team = tid / TPE;
+    const int lt = tid - team * TPE;
+    const int loc = lt % N2;
+    const int h = lt / N2;
+    const int i = loc % N;
+    const int j = loc / N;
+    const int nvalid = min(EPB, P.nelt - e0);
+    const int e = e0 + team;
+    const bool active = team < nvalid;
+    const long long S = P.stride;
+
+    const TC* s_uc;
+    if constexpr (F32) {
+        // FP32 copy of the tile as deviations from the element's centre node: the
+        // derivatives are unchanged (rows of D sum to zero) and the rounding error
+        // scales with the variation across the element instead of |u|
+        TC* w = reinterpret_cast<TC*>(smem_uc);
+        constexpr int centre = (N / 2) * (1 + RP + PP);
+        const int cnt = tid < NT ? nvalid * EN3 : 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            for (int x = tid; x < cnt; x += NT) {
+                const double ref = su[c * CS + (x / EN3) * EN3 + centre];
+                w[c * CS + x] = static_cast<float>(su[c * CS + x] - ref);
+            }
+        s_uc = w;
+    } else {
+        s_uc = reinterpret_cast<const TC*>(su);
+    }
+
+    // ---- face phase ---------------------------------------------------------------
+    face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY>(P, e0, su, sg, sc, sflux, tid, G);
     __syncthreads();
 
     // ---- column phase: volume curl + face terms + LSRK update ------------------
