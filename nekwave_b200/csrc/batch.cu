@@ -29,7 +29,7 @@ template <> struct BShape<5> { static constexpr int KS = 2, EPB = 2, ALG = 4; };
 template <> struct BShape<6> { static constexpr int KS = 2, EPB = 1, ALG = 4; };
 template <> struct BShape<7> { static constexpr int KS = 2, EPB = 1, ALG = 4; };
 template <> struct BShape<8> { static constexpr int KS = 2, EPB = 1, ALG = 8; };
-template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1, ALG = 0; };
+template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1, ALG = 4; };
 template <> struct BShape<10> { static constexpr int KS = 1, EPB = 1, ALG = 0; };
 
 template <int N, bool F32>
@@ -43,9 +43,11 @@ constexpr int bsmem() {
 // geometry, connections), wait, compute.  Threads beyond the shape's count take
 // part in the barriers only.
 template <int N, bool F32, int KS, int EPB, int ALG>
-__device__ __forceinline__ void tile2(const StageParams& P, int e0, unsigned char* smem, int tid) {
+__device__ __forceinline__ void tile2(const StageParams& P, int e0, unsigned char* smem, int tid,
+                                      const double* Dc = nullptr) {
     constexpr bool SPLIT = ((ALG - 2) & 2) != 0, PAD = ((ALG - 2) & 4) != 0;
-    static_assert(((ALG - 2) & 1) == 0, "one tile per call");
+    constexpr bool CONSTD = ((ALG - 2) & 8) != 0;
+    static_assert(((ALG - 2) & 1) == 0 && ((ALG - 2) & 16) == 0, "one tile per call, tile resident");
     using L2 = stage::Layout2<N, F32, EPB, false, PAD>;
     constexpr int NT = EPB * KS * N * N;
     double* sD = reinterpret_cast<double*>(smem + L2::D);
@@ -60,9 +62,9 @@ __device__ __forceinline__ void tile2(const StageParams& P, int e0, unsigned cha
     stage::cp_async_wait<0>();
     __syncthreads();
     stage::FaceGather<stage::face_points_per_thread<N, KS>()> G;
-    stage::compute2<N, GEO_BOX, F32, KS, EPB, SPLIT, PAD>(P, e0, su, sg, sc, sD,
-                                                          reinterpret_cast<double*>(smem + L2::flux),
-                                                          smem + L2::uc, tid, G);
+    stage::compute2<N, GEO_BOX, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, e0, su, sg, sc, sD,
+                                                                  reinterpret_cast<double*>(smem + L2::flux),
+                                                                  smem + L2::uc, tid, G, Dc);
 }
 
 template <int N, bool F32>
@@ -87,7 +89,7 @@ __constant__ double c_rk4b[5] = {1432997174477.0 / 9575080441755.0,
                                  2277821191437.0 / 14882151754819.0};
 
 template <bool F32>
-__global__ void __launch_bounds__(kBatchThreads, 4)
+__global__ void __launch_bounds__(kBatchThreads, 3)
 batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
                    const int* __restrict__ ntiles_p, int* __restrict__ counters, int stage, int dry) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -167,14 +169,20 @@ __device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, 
     return P;
 }
 
+// D of one N by value, for the constant-bank form of the per-N kernels.
+struct DParam {
+    double d[100];
+};
+
 // One block per tile of one N: the single-mesh kernel's tuned shape for that N,
 // fully unrolled, reading its slot from the work item (per-N mode).  ALG 0 is the
-// first-family tile (stage_kernel.cuh); ALG 2 + flags (SPLIT = 2, PAD = 4, no
-// PIPE: the work list is walked one tile per block) the second (stage_pipe.cuh).
+// first-family tile (stage_kernel.cuh); ALG 2 + flags (SPLIT = 2, PAD = 4,
+// CONSTD = 8 with D from dp; no PIPE: the work list is walked one tile per block)
+// the second (stage_pipe.cuh).
 template <int N, bool F32, int KS, int EPB, bool KSMEM, int MINB, int ALG>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
 batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work,
-                     int stage, int dry) {
+                     int stage, int dry, const __grid_constant__ DParam dp) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WorkItem w = work[blockIdx.x];
     const SlotDev& S = slots[w.slot];
@@ -183,32 +191,33 @@ batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restri
     if constexpr (ALG == 0)
         stage_tile<N, GEO_BOX, F32, KS, EPB, KSMEM, true>(P, w.e0, smem, threadIdx.x);
     else
-        tile2<N, F32, KS, EPB, ALG>(P, w.e0, smem, threadIdx.x);
+        tile2<N, F32, KS, EPB, ALG>(P, w.e0, smem, threadIdx.x, dp.d);
 }
 
 // Per-N shapes of the per-N mode: the single-mesh defaults (stage_variants.h entry
 // 0), with the persistent form of N = 4 replaced by its one-tile-per-block form.
+// An ALG with CONSTD runs without it for an N whose cavities do not all share the
+// pool's D for that N (same arithmetic, D from shared memory).
 template <int N> struct NShape;
 template <> struct NShape<2> { static constexpr int KS = 2, EPB = 16, KSM = 1, MINB = 1, ALG = 0; };
 template <> struct NShape<3> { static constexpr int KS = 1, EPB = 16, KSM = 0, MINB = 4, ALG = 0; };
-template <> struct NShape<4> { static constexpr int KS = 2, EPB = 4, KSM = 0, MINB = 4, ALG = 4; };
+template <> struct NShape<4> { static constexpr int KS = 2, EPB = 4, KSM = 0, MINB = 4, ALG = 12; };
 template <> struct NShape<5> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 4, ALG = 4; };
 template <> struct NShape<6> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 3, ALG = 4; };
 template <> struct NShape<7> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 4; };
-template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 8; };
-template <> struct NShape<9> { static constexpr int KS = 3, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
+template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 12; };
+template <> struct NShape<9> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 4; };
 template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
 
-template <int N, bool F32>
-cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
-                     cudaStream_t st, int* epb_out) {
+template <int N, bool F32, int ALG>
+cudaError_t launch_n_alg(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
+                         const DParam& dp, cudaStream_t st) {
     using Sh = NShape<N>;
     constexpr int threads = Sh::EPB * Sh::KS * N * N;
-    constexpr int smem = Sh::ALG == 0
+    constexpr int smem = ALG == 0
         ? SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total
-        : stage::Layout2<N, F32, Sh::EPB, false, (((Sh::ALG - 2) & 4) != 0)>::total;
-    auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB, Sh::ALG>;
-    if (epb_out) *epb_out = Sh::EPB;
+        : stage::Layout2<N, F32, Sh::EPB, false, (((ALG - 2) & 4) != 0)>::total;
+    auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB, ALG>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -216,8 +225,32 @@ cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int 
         attr_set = true;
     }
     if (ntiles <= 0) return cudaSuccess;
-    kern<<<ntiles, threads, smem, st>>>(slots, work, stage, dry);
+    kern<<<ntiles, threads, smem, st>>>(slots, work, stage, dry, dp);
     return cudaGetLastError();
+}
+
+// Dh: this N's D on the host when every resident cavity of this N uses it (the
+// constant-bank form then applies), else null.
+template <int N, bool F32>
+cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
+                     const double* Dh, cudaStream_t st, int* epb_out) {
+    using Sh = NShape<N>;
+    if (epb_out) *epb_out = Sh::EPB;
+    constexpr bool cd_bit = Sh::ALG >= 2 && ((Sh::ALG - 2) & 8) != 0;
+    constexpr bool has_cd = cd_bit && !F32;  // the constant-bank D is an FP64 form
+    constexpr int ALG_PLAIN = cd_bit ? Sh::ALG - 8 : Sh::ALG;
+    DParam dp{};
+    if constexpr (has_cd) {
+        if (Dh) {
+            for (int x = 0; x < N * N; ++x) dp.d[x] = Dh[x];
+            return launch_n_alg<N, F32, Sh::ALG>(stage, slots, work, ntiles, dry, dp, st);
+        }
+        if (ntiles <= 0) {  // set-up call: prepare both forms
+            cudaError_t e = launch_n_alg<N, F32, Sh::ALG>(stage, slots, work, 0, dry, dp, st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return launch_n_alg<N, F32, ALG_PLAIN>(stage, slots, work, ntiles, dry, dp, st);
 }
 
 // Does this slot record energy after the step it is taking now (post = 1), or
@@ -358,11 +391,12 @@ int max_batch_smem() {
 }  // namespace
 
 cudaError_t launch_batch_stage_n(int N, int f32, int stage, const SlotDev* slots,
-                                 const WorkItem* work, int ntiles, int dry, cudaStream_t st) {
+                                 const WorkItem* work, int ntiles, int dry, const double* Dh,
+                                 cudaStream_t st) {
     switch (N) {
 #define NWB_CASE(n) \
-        case n: return f32 ? launch_n<n, true>(stage, slots, work, ntiles, dry, st, nullptr) \
-                           : launch_n<n, false>(stage, slots, work, ntiles, dry, st, nullptr);
+        case n: return f32 ? launch_n<n, true>(stage, slots, work, ntiles, dry, Dh, st, nullptr) \
+                           : launch_n<n, false>(stage, slots, work, ntiles, dry, Dh, st, nullptr);
         NWB_CASE(2) NWB_CASE(3) NWB_CASE(4) NWB_CASE(5) NWB_CASE(6) NWB_CASE(7) NWB_CASE(8)
         NWB_CASE(9) NWB_CASE(10)
 #undef NWB_CASE

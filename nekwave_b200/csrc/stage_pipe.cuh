@@ -12,7 +12,8 @@
 //          into L2.  Without PIPE a block computes one tile, as stage_tile does.
 //   SPLIT  (KS = 2) the two threads of a node column split the residual by field
 //          instead of by planes: thread h = 0 forms the E residual (curl H) and
-//          h = 1 the H residual (-curl E), each for all N planes.  The components
+//          h = 1 the H residual (-curl E), each for all N planes (KS = 1: one thread
+//          forms both, one after the other, with the same arithmetic).  The components
 //          a thread differentiates along t are read once per column into
 //          registers, so shared memory serves only the r and s derivatives, and
 //          each thread lifts, updates and stores three components.
@@ -20,8 +21,9 @@
 //          an element at i + (N+1)(j + N k)), which spreads the traces of the
 //          r-faces (i = 0, N-1) and the rows of the r-derivative over the banks.
 //   CONSTD (with SPLIT, FP64) the plane loop is unrolled, so the t-derivative's
-//          D(k,l) are compile-time indices into the kernel's parameter copy of D
-//          and enter the FMAs as constant-bank operands instead of shared loads.
+//          D(k,l) are compile-time indices into a kernel-parameter copy of D (Dc,
+//          StageParams::Dc or the pool's per-N parameter) and enter the FMAs as
+//          constant-bank operands instead of shared loads.
 //   EARLY  (without PIPE) the neighbour traces of the tile's face points are
 //          requested from global memory right after the tile's copies are issued,
 //          before the block waits for them, so both latencies overlap.  On a
@@ -336,7 +338,8 @@ template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool 
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
-                                         FaceGather<face_points_per_thread<N, KS>()>& G) {
+                                         FaceGather<face_points_per_thread<N, KS>()>& G,
+                                         const double* __restrict__ Dc = nullptr) {
     using TC = typename std::conditional<F32, float, double>::type;
     constexpr int N2 = N * N, N3 = N2 * N;
     constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
@@ -346,7 +349,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     constexpr int NT = EPB * TPE;
     constexpr int KPT = (N + KS - 1) / KS;
     constexpr int CS = EPB * EN3;
-    static_assert(!SPLIT || KS == 2, "the field split needs two threads per column");
+    static_assert(!SPLIT || KS == 1 || KS == 2, "the field split: one or two threads per column");
     static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
 
     const int team = tid / TPE;
@@ -403,10 +406,14 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     const long long ebase = static_cast<long long>(e) * N3;
 
     if constexpr (SPLIT) {
-        // thread h = 0: E residual from V = H (+curl H); h = 1: H residual from V = E (-curl E)
-        const int src = h == 0 ? 3 : 0;
+        // field hf = 0: E residual from V = H (+curl H); hf = 1: H residual from V = E
+        // (-curl E).  KS = 2: thread h takes field h; KS = 1: one thread takes both,
+        // one after the other, with the same arithmetic per node.
+#pragma unroll 1
+        for (int hf = (KS == 2 ? h : 0); hf < (KS == 2 ? h + 1 : 2); ++hf) {
+        const int src = hf == 0 ? 3 : 0;
         const int dst = 3 - src;
-        const double sgn = h == 0 ? 1.0 : -1.0;
+        const double sgn = hf == 0 ? 1.0 : -1.0;
         const TC* V = U + src * CS;
         constexpr int NC = GEO == GEO_BOX ? 2 : 3;  // components differentiated along t
         TC col[NC][N];
@@ -428,7 +435,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TC dr = Dr[l], ds = Ds[l];
-                    const TC dt = CONSTD ? static_cast<TC>(P.Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
+                    const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
                     Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
@@ -444,7 +451,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TC dr = Dr[l], ds = Ds[l];
-                    const TC dt = CONSTD ? static_cast<TC>(P.Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
+                    const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
 #pragma unroll
@@ -481,6 +488,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 __stcs(P.k + (dst + c) * S + g, kn);
                 __stcs(P.u_out + (dst + c) * S + g, Uf[(dst + c) * CS + ms] + B * kn);
             }
+        }
         }
     } else {
         // one plane at a time: the register budget goes to the batched loads
@@ -577,7 +585,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
           bool CONSTD, bool EARLY>
-__global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const StageParams P) {
+__global__ void __launch_bounds__(EPB * KS * N * N, MINB)
+    stage2_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using L = Layout2<N, F32, EPB, PIPE, PAD>;
     constexpr int NT = EPB * KS * N * N;
@@ -600,7 +609,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
         cp_async_wait<0>();
         __syncthreads();
         compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY>(P, t * EPB, su(0), sg(0), sc(0), sD,
-                                                                  sflux, smem + L::uc, tid, G);
+                                                                  sflux, smem + L::uc, tid, G, P.Dc);
     } else {
         for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
             const int b = n & 1;
@@ -610,7 +619,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB) stage2_kernel(const St
             if (tn < ntiles) issue2<N, GEO, EPB, NT, PAD>(P, tn * EPB, su(b ^ 1), sg(b ^ 1), sc(b ^ 1), tid);
             cp_async_commit();
             compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
-                                                               smem + L::uc, tid, G);
+                                                               smem + L::uc, tid, G, P.Dc);
         }
         cp_async_wait<0>();
     }

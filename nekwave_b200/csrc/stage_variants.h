@@ -13,7 +13,8 @@
 // 16 = EARLY (without PIPE: neighbour traces requested before the tile wait).
 // Entry 0 is the default for every geometry class (the fastest FP64 shape on B200
 // in a sweep over 8 M-node box meshes); the autotuner (nwb_solver_autotune) times
-// them all for the axis-aligned class on the caller's own mesh.
+// them all for the axis-aligned class on the caller's own mesh.  The pool's per-N
+// kernels (batch.cu NShape/BShape) use the same arithmetic as entry 0.
 #pragma once
 
 #define NWB_VARIANTS_2(X) X(2, 16, 1, 1, 0) X(2, 32, 0, 2, 0) X(1, 32, 0, 2, 0)
@@ -23,5 +24,5 @@
 #define NWB_VARIANTS_6(X) X(2, 2, 0, 3, 4) X(2, 2, 0, 3, 0) X(2, 2, 1, 1, 0) X(3, 2, 0, 2, 0) X(6, 1, 0, 2, 0) X(2, 4, 0, 1, 0) X(6, 1, 0, 3, 3) X(2, 2, 0, 3, 8) X(2, 2, 0, 3, 5) X(2, 2, 0, 3, 9) X(2, 4, 0, 2, 4) X(2, 2, 0, 3, 12) X(2, 2, 0, 3, 16) X(2, 2, 0, 4, 4) X(2, 2, 0, 5, 4) X(2, 4, 0, 2, 12) X(2, 2, 0, 3, 20) X(2, 2, 0, 3, 28)
 #define NWB_VARIANTS_7(X) X(2, 1, 0, 4, 4) X(1, 2, 0, 3, 0) X(1, 2, 1, 1, 0) X(7, 1, 0, 2, 0) X(1, 4, 0, 1, 0) X(2, 2, 0, 3, 4) X(2, 2, 0, 3, 8) X(2, 1, 0, 4, 12) X(2, 1, 0, 5, 4) X(2, 1, 0, 6, 4) X(2, 1, 0, 4, 20)
 #define NWB_VARIANTS_8(X) X(2, 1, 0, 4, 12) X(2, 1, 0, 4, 8) X(2, 1, 0, 4, 0) X(2, 1, 1, 1, 0) X(4, 1, 0, 2, 0) X(8, 1, 0, 1, 0) X(1, 2, 0, 2, 0) X(2, 2, 0, 2, 0) X(4, 1, 0, 2, 3) X(2, 1, 0, 4, 4) X(2, 1, 0, 3, 5) X(2, 1, 0, 3, 9) X(2, 1, 0, 4, 6) X(2, 1, 0, 4, 16) X(2, 1, 0, 4, 28) X(2, 1, 0, 4, 20) X(1, 1, 0, 5, 40) X(2, 1, 0, 3, 1)
-#define NWB_VARIANTS_9(X) X(3, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(9, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8)
-#define NWB_VARIANTS_10(X) X(2, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(5, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8)
+#define NWB_VARIANTS_9(X) X(2, 1, 0, 2, 4) X(3, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(9, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8) X(2, 1, 0, 2, 12) X(2, 1, 0, 3, 12)
+#define NWB_VARIANTS_10(X) X(2, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(5, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8) X(2, 1, 0, 2, 4) X(2, 1, 0, 2, 12)

@@ -45,3 +45,45 @@ def test_reference_cli_case_on_nwb(gpu, tmp_path):
     energies = [float(x[-1]) for x in rows[1:]]
     assert len(energies) >= 8
     assert all(b <= a * (1 + 1e-12) for a, b in zip(energies, energies[1:]))  # upwind decays
+
+
+REF_CLI = os.path.join(ROOT, "oracle", "_ref", "nekwave-ref")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CLI), reason="reference CLI not built")
+def test_reference_cli_end_to_end_against_dropin(gpu, tmp_path):
+    """The same case through the reference's own CLI and CUDA path (oracle/_ref,
+    built from its sources) and through the drop-in CLI on libnwb: the benchmark
+    workload (periodic 32^3, 8 points, central), 50 steps of Case::simulate with its
+    per-step download, host probes and energy.  The CLI has no way to choose an
+    initial wave (the reference ignores wave_type in a case file), so the fields
+    start at zero and the run times the full Case::simulate loop; the energy
+    histories must agree.  Wall times are recorded (gpurun_out/cli_e2e.json)."""
+    import time
+    case = {"mesh": {"nelx": 32, "nely": 32, "nelz": 32, "xmin": 0.0, "xmax": 1.0, "ymin": 0.0,
+                     "ymax": 1.0, "zmin": 0.0, "zmax": 1.0, "periodic": "all"},
+            "numerics": {"order": 8, "cfl": 0.5, "flux_type": "central"},
+            "time": {"num_steps": 50},
+            "output": {"output_frequency": 10, "export_fields": False, "export_format": "csv"}}
+    out = {}
+    for name, exe in (("reference", REF_CLI), ("dropin", os.path.join(DROPIN, "nekwave"))):
+        d = tmp_path / name
+        d.mkdir()
+        c = dict(case)
+        c["output"] = dict(case["output"], output_dir=str(d / "out"))
+        p = d / "case.json"
+        p.write_text(json.dumps(c))
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, str(p)], capture_output=True, text=True, timeout=900, cwd=d)
+        wall = time.perf_counter() - t0
+        assert r.returncode == 0, name + ": " + r.stdout[-2000:] + r.stderr[-2000:]
+        rows = list(csv.reader(open(d / "out" / "energy_history.csv")))
+        out[name] = dict(wall_s=wall, energies=[float(x[-1]) for x in rows[1:]])
+    a, b = out["reference"]["energies"], out["dropin"]["energies"]
+    assert len(a) == len(b) >= 5
+    assert all(abs(x - y) <= 1e-10 * abs(x) for x, y in zip(a, b))
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    with open(os.path.join(ROOT, "gpurun_out", "cli_e2e.json"), "w") as f:
+        json.dump({"case": "periodic 32^3, 8 points, central, 50 steps, Case::simulate",
+                   "reference_wall_s": out["reference"]["wall_s"],
+                   "dropin_wall_s": out["dropin"]["wall_s"]}, f)

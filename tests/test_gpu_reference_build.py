@@ -73,13 +73,17 @@ def test_random_state_matches_reference_cuda_build(gpu, N, nel, per, c0):
     s.finalize()
 
 
-def test_reference_cuda_step_time_on_benchmark_workload(gpu):
-    """Times the reference's own DgSolver::step on the benchmark workload (periodic
-    32^3, 8 points, central) and records it next to ours (gpurun_out/)."""
-    N, nel, per = 8, (32, 32, 32), (1, 1, 1)
+@pytest.mark.parametrize("name,N,nel,lo,hi,per,c0", [
+    ("c1", 5, (4, 4, 4), (0, 0, 0), (1, 1, 1), (0, 0, 0), 1.0),
+    ("c2", 8, (32, 32, 32), (0, 0, 0), (1, 1, 1), (1, 1, 1), 0.0),
+    ("c3", 6, (64, 64, 32), (0, 0, 0), (2, 2, 1), (0, 0, 0), 1.0)])
+def test_reference_cuda_step_time(gpu, name, N, nel, lo, hi, per, c0):
+    """Times the reference's own DgSolver::step (CUDA events around 10 steps after 3
+    warm-up steps, no per-step download) on the benchmark workloads and records it
+    next to ours (gpurun_out/ref_gpu_timing_<name>.json)."""
     L = O.ref_gpu()
-    mh = L.nwref_mesh_box(N, *nel, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, *per)
-    s = L.nwref_gpu_create(mh, 0.0)
+    mh = L.nwref_mesh_box(N, *nel, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], *per)
+    s = L.nwref_gpu_create(mh, c0)
     npts = nel[0] * nel[1] * nel[2] * N ** 3
     u = np.zeros(6 * npts)
     L.nwref_gpu_upload(s, O._dp(u), u.size)
@@ -90,7 +94,7 @@ def test_reference_cuda_step_time_on_benchmark_workload(gpu):
     L.nwref_mesh_free(mh)
     rate = 6 * npts * 5 * 10 / (ms / 1e3) / 1e9
     os.makedirs(OUT, exist_ok=True)
-    with open(os.path.join(OUT, "ref_gpu_timing.json"), "w") as f:
-        json.dump({"workload": "periodic 32^3 N=8 central", "ms_per_step": ms / 10,
+    with open(os.path.join(OUT, f"ref_gpu_timing_{name}.json"), "w") as f:
+        json.dump({"workload": name, "N": N, "nel": list(nel), "ms_per_step": ms / 10,
                    "gdof_stage_per_s": rate}, f)
     assert rate > 0
