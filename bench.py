@@ -65,6 +65,23 @@ def workload_spec(name, nel_override, seed):
 L2_BYTES = 126 * 1024 * 1024
 
 
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """Largest value of x over all ranks (the job's time is its slowest rank's);
+    x itself without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(dof_stages_per_rank: float, seconds_max: float, world: int) -> float:
+    """Whole-job GDOF-stage/s: every rank's DOF-stages over the slowest rank's time."""
+    return dof_stages_per_rank * world / seconds_max / 1e9
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -460,12 +477,8 @@ def main():
         barrier()
     launches = solver.launchCount() - launches0
     clocks = clk.summary()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist_on:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    dof_stage = 6 * npts * 5 * args.steps * world
-    value = dof_stage / (ms_max / 1e3) / 1e9
+    ms_max = max_over_ranks(ms)
+    value = job_rate(6 * npts * 5 * args.steps, ms_max / 1e3, world)
 
     # ---- roofline of the fused stage kernel (CUDA events on the solver's stream) ----------
     stage_ms = solver.timeStageKernel(dt, 50)
@@ -492,10 +505,7 @@ def main():
         solver.downloadState(hnp)          # D2H of the step's result state
     barrier()
     e2e_sec = time.perf_counter() - t0
-    tt = torch.tensor([e2e_sec], dtype=torch.float64, device="cuda")
-    if dist_on:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = 6 * npts * 5 * e2e_steps * world / float(tt.item()) / 1e9
+    e2e_value = job_rate(6 * npts * 5 * e2e_steps, max_over_ranks(e2e_sec), world)
     del ctypes, ev0
 
     accuracy = None

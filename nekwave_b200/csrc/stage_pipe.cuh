@@ -24,6 +24,10 @@
 //          D(k,l) are compile-time indices into a kernel-parameter copy of D (Dc,
 //          StageParams::Dc or the pool's per-N parameter) and enter the FMAs as
 //          constant-bank operands instead of shared loads.
+//   FACEFIRST (without PIPE) the whole face phase runs from global memory (own and
+//          neighbour traces, connections, normals and lifts through the read-only
+//          path) while the tile's copies are in flight; the column phase follows
+//          the wait.  The face phase's latency then overlaps the tile's.
 //   EARLY  (without PIPE) the neighbour traces of the tile's face points are
 //          requested from global memory right after the tile's copies are issued,
 //          before the block waits for them, so both latencies overlap.  On a
@@ -333,8 +337,79 @@ __device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, 
     }
 }
 
+// Face phase from global memory only: own and neighbour traces, connections (or
+// the box structure), normals and lifts, so that it runs while the tile's copies
+// are in flight.  Writes the lifted fluxes into sflux like face_phase2; the caller
+// synchronises after waiting for the tile.
+template <int N, int GEO, bool F32, int KS, int EPB>
+__device__ __forceinline__ void face_phase_global(const StageParams& P, const int e0, double* sflux,
+                                                  const int tid) {
+    using TC = typename std::conditional<F32, float, double>::type;
+    constexpr int N2 = N * N, N3 = N2 * N;
+    constexpr int TPE = KS * N2;
+    constexpr int FPT = face_points_per_thread<N, KS>();
+    const int team = tid / TPE;
+    const int lt = tid - team * TPE;
+    const int e = e0 + team;
+    if (team >= min(EPB, P.nelt - e0)) return;
+    const long long S = P.stride;
+    FaceGather<FPT> G;
+    gather2<N, GEO, KS, EPB, false, false>(P, e0, nullptr, nullptr, tid, G);
+    double own[FPT][6];
+#pragma unroll
+    for (int q = 0; q < FPT; ++q) {
+        const int fp = lt + q * TPE;
+        if (fp < 6 * N2) {
+            const int f = fp / N2;
+            const int pq = fp - f * N2;
+            const long long g = static_cast<long long>(e) * N3 + face_local<N>(f, pq % N, pq / N);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) own[q][c] = __ldg(P.u_in + c * S + g);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < FPT; ++q) {
+        const int fp = lt + q * TPE;
+        if (fp >= 6 * N2) break;
+        const int f = fp / N2;
+        const int pq = fp - f * N2;
+        double nxd, nyd, nzd, lift;
+        if constexpr (GEO == GEO_NODAL) {
+            const long long gf = (static_cast<long long>(e) * 6 + f) * N2 + pq;
+            nxd = __ldg(P.fnrm + gf);
+            nyd = __ldg(P.fnrm + P.nfp + gf);
+            nzd = __ldg(P.fnrm + 2 * P.nfp + gf);
+            lift = __ldg(P.flift + gf);
+        } else {
+            const ElemGeo* Gp = P.geo + e;
+            nxd = __ldg(&Gp->nrm[f][0]);
+            nyd = __ldg(&Gp->nrm[f][1]);
+            nzd = __ldg(&Gp->nrm[f][2]);
+            lift = __ldg(&Gp->lift[f]);
+        }
+        double jmp[6];
+        if (G.vB[q] < 0) {
+            // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
+            jmp[0] = -2.0 * own[q][0]; jmp[1] = -2.0 * own[q][1]; jmp[2] = -2.0 * own[q][2];
+            jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) jmp[c] = G.nb[q][c] - own[q][c];
+        }
+        TC fl[6];
+        numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
+                           static_cast<TC>(0.5 * P.c0), static_cast<TC>(jmp[0]),
+                           static_cast<TC>(jmp[1]), static_cast<TC>(jmp[2]),
+                           static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
+                           static_cast<TC>(jmp[5]), fl);
+        double* F = sflux + (team * 6 + f) * 6 * N2 + pq;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
+    }
+}
+
 template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
-          bool EARLY = false>
+          bool EARLY = false, bool FACEDONE = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
@@ -382,8 +457,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
         s_uc = reinterpret_cast<const TC*>(su);
     }
 
-    // ---- face phase ---------------------------------------------------------------
-    face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY>(P, e0, su, sg, sc, sflux, tid, G);
+    // ---- face phase (unless the caller ran it from global memory) -------------------
+    if constexpr (!FACEDONE) face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY>(P, e0, su, sg, sc, sflux, tid, G);
     __syncthreads();
 
     // ---- column phase: volume curl + face terms + LSRK update ------------------
@@ -584,7 +659,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 }
 
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD, bool EARLY>
+          bool CONSTD, bool EARLY, bool FACEFIRST>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage2_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -600,16 +675,17 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     auto su = [&](int b) { return reinterpret_cast<double*>(smem + L::u0 + b * L::tile); };
     auto sg = [&](int b) { return reinterpret_cast<ElemGeo*>(smem + L::geo0 + b * L::geo_b); };
     auto sc = [&](int b) { return reinterpret_cast<int*>(smem + L::conn0 + b * L::conn_b); };
-    static_assert(!(EARLY && PIPE), "the early gather belongs to the one-tile form");
+    static_assert(!((EARLY || FACEFIRST) && PIPE), "early forms belong to the one-tile form");
     FaceGather<face_points_per_thread<N, KS>()> G;
     issue2<N, GEO, EPB, NT, PAD>(P, t * EPB, su(0), sg(0), sc(0), tid);
     cp_async_commit();
     if constexpr (!PIPE) {
-        if constexpr (EARLY) gather2<N, GEO, KS, EPB, PAD, false>(P, t * EPB, nullptr, nullptr, tid, G);
+        if constexpr (FACEFIRST) face_phase_global<N, GEO, F32, KS, EPB>(P, t * EPB, sflux, tid);
+        else if constexpr (EARLY) gather2<N, GEO, KS, EPB, PAD, false>(P, t * EPB, nullptr, nullptr, tid, G);
         cp_async_wait<0>();
         __syncthreads();
-        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY>(P, t * EPB, su(0), sg(0), sc(0), sD,
-                                                                  sflux, smem + L::uc, tid, G, P.Dc);
+        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY, FACEFIRST>(
+            P, t * EPB, su(0), sg(0), sc(0), sD, sflux, smem + L::uc, tid, G, P.Dc);
     } else {
         for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
             const int b = n & 1;
@@ -629,11 +705,11 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
 // at once (queried with the occupancy calculator on the first call, which the
 // solver makes at creation, outside any stream capture), never more than tiles.
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD, bool EARLY>
+          bool CONSTD, bool EARLY, bool FACEFIRST>
 cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int threads = EPB * KS * N * N;
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
-    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY>;
+    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY, FACEFIRST>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
     static int resident = 0;
     if (resident == 0) {
