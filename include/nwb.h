@@ -140,6 +140,26 @@ nwb_status nwb_eval_rhs(nwb_solver* s, double* host_rhs, size_t n);
  * FP64, on the device (src/case.cpp:733-766).  Returns NWB_ENONFINITE (and the
  * non-finite energy) when the state holds NaN/Inf. */
 nwb_status nwb_energy(nwb_solver* s, double* energy);
+/* Point probes on the device: ProbeManager::init's data (src/probe.cpp:33-96) --
+ * per probe the first node of its element (e*N^3) and its N^3 tensor Lagrange
+ * weights -- replace any earlier set; nprobes = 0 removes them. */
+nwb_status nwb_probe_setup(nwb_solver* s, int nprobes, const long long* node_offset,
+                           const double* weights /* [nprobes][N^3] */);
+/* ProbeManager::record (src/probe.cpp:192-216) on the current state, on the
+ * device, with the reference's summation order and roundings: out[p*6 + c] for
+ * c = Ex, Ey, Ez, Hx, Hy, Hz.  Synchronous; the reference computes these on the
+ * host from a full download of the state every step (src/case.cpp:588-600). */
+nwb_status nwb_probe_read(nwb_solver* s, double* out);
+/* Asynchronous snapshot of the current state into host memory (6*npts doubles, in
+ * the reference's [6][npts] layout; pinned memory lets the copy overlap later
+ * steps).  The state is first copied on the device in stream order, after every
+ * step already queued, so steps queued afterwards may run while the host copy is
+ * in flight; nwb_snapshot_wait returns when the host buffer is complete.  One
+ * snapshot is in flight at a time (a second begin waits for the first).  Replaces
+ * the synchronous per-step download of Case::simulate (src/case.cpp:588) where
+ * the caller only needs the state at save steps. */
+nwb_status nwb_snapshot_begin(nwb_solver* s, double* host, size_t n);
+nwb_status nwb_snapshot_wait(nwb_solver* s);
 nwb_status nwb_solver_destroy(nwb_solver* s);
 
 /* Introspection used by tests and the benchmark. */

@@ -77,6 +77,10 @@ SIGNATURES = {
     "nwb_sync": (C.c_int, [C.c_void_p]),
     "nwb_eval_rhs": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_energy": (C.c_int, [C.c_void_p, _D]),
+    "nwb_probe_setup": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _D]),
+    "nwb_probe_read": (C.c_int, [C.c_void_p, _D]),
+    "nwb_snapshot_begin": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
+    "nwb_snapshot_wait": (C.c_int, [C.c_void_p]),
     "nwb_solver_destroy": (C.c_int, [C.c_void_p]),
     "nwb_solver_get_info": (C.c_int, [C.c_void_p, C.POINTER(SolverInfo)]),
     "nwb_solver_device_state": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(C.c_void_p)]),

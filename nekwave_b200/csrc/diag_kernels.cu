@@ -52,6 +52,23 @@ __global__ void energy_final_kernel(const double* __restrict__ partial, int n,
     }
 }
 
+// ProbeManager::record (src/probe.cpp:192-216): thread (probe, component) sums
+// w[p] * u[offset + p] over the probe element's N^3 nodes in node order, with
+// separate multiply and add roundings as on the host, so the values equal the
+// reference's bit for bit on the same state and weights.
+__global__ void probe_kernel(const double* __restrict__ u, long long stride, int N3,
+                             const long long* __restrict__ offset, const double* __restrict__ w,
+                             int nprobes, double* __restrict__ out) {
+    const int pr = blockIdx.x;
+    const int c = threadIdx.x;
+    if (pr >= nprobes || c >= 6) return;
+    const double* wp = w + static_cast<long long>(pr) * N3;
+    const double* up = u + c * stride + offset[pr];
+    double acc = 0.0;
+    for (int p = 0; p < N3; ++p) acc = __dadd_rn(acc, __dmul_rn(wp[p], up[p]));
+    out[pr * 6 + c] = acc;
+}
+
 __global__ void l2_flush_kernel(int4* __restrict__ buf, size_t n16) {
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
     for (size_t x = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; x < n16; x += stride)
@@ -75,6 +92,13 @@ cudaError_t launch_energy(const double* u, long long stride, int N, int nelt,
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     energy_final_kernel<<<1, 32, 0, st>>>(partial, nblocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probes(const double* u, long long stride, int N3, const long long* offset,
+                          const double* w, int nprobes, double* out, cudaStream_t st) {
+    if (nprobes <= 0) return cudaSuccess;
+    probe_kernel<<<nprobes, 32, 0, st>>>(u, stride, N3, offset, w, nprobes, out);
     return cudaGetLastError();
 }
 

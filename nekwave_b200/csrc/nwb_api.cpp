@@ -213,6 +213,16 @@ struct nwb_solver {
     double hD[100] = {};
     int snel[3] = {0, 0, 0};  // structured box mesh (x-fastest elements), 0 = not
     int spmask = 0;
+    // probes (nwb_probe_setup): node offset and N^3 weights per probe, device values
+    int nprobes = 0;
+    long long* dprobe_off = nullptr;
+    double* dprobe_w = nullptr;
+    double* dprobe_out = nullptr;
+    // asynchronous snapshots (nwb_snapshot_begin/wait)
+    double* dsnap = nullptr;
+    cudaStream_t snap_st = nullptr;
+    cudaEvent_t snap_ev = nullptr;
+    bool snap_pending = false;
     nwb::ElemGeo* dgeo = nullptr;
     int* dconn = nullptr;
     double* djac_e = nullptr;
@@ -341,11 +351,15 @@ struct nwb_solver {
     void release() {
         drop_graphs();
         void* ptrs[] = {u[0], u[1], k, dD, dgeo, dconn, djac_e, dmet_n, dfnrm, dflift,
-                        dfplus, djac_n, dw3, dpartial, denergy, dflush};
+                        dfplus, djac_n, dw3, dpartial, denergy, dflush, dprobe_off, dprobe_w, dprobe_out, dsnap};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
         st = nullptr;
+        if (snap_st) cudaStreamDestroy(snap_st);
+        snap_st = nullptr;
+        if (snap_ev) cudaEventDestroy(snap_ev);
+        snap_ev = nullptr;
     }
 };
 
@@ -702,9 +716,82 @@ nwb_status nwb_energy(nwb_solver* s, double* out) {
     return NWB_OK;
 }
 
+nwb_status nwb_probe_setup(nwb_solver* s, int nprobes, const long long* node_offset,
+                           const double* weights) {
+    if (!s) return fail(NWB_EINVAL, "nwb_probe_setup: null solver");
+    if (nprobes < 0 || (nprobes > 0 && (!node_offset || !weights)))
+        return fail(NWB_EINVAL, "nwb_probe_setup: bad probe arrays");
+    const int N3 = s->N * s->N * s->N;
+    for (int p = 0; p < nprobes; ++p)
+        if (node_offset[p] < 0 || node_offset[p] % N3 != 0 || node_offset[p] + N3 > s->npts)
+            return fail(NWB_EINVAL, "nwb_probe_setup: probe %d offset %lld is not an element start", p,
+                        node_offset[p]);
+    NWB_CU(cudaStreamSynchronize(s->st));
+    for (void* q : {static_cast<void*>(s->dprobe_off), static_cast<void*>(s->dprobe_w),
+                    static_cast<void*>(s->dprobe_out)})
+        if (q) cudaFree(q);
+    s->dprobe_off = nullptr;
+    s->dprobe_w = nullptr;
+    s->dprobe_out = nullptr;
+    s->nprobes = 0;
+    if (nprobes == 0) return NWB_OK;
+    NWB_CU(cudaMalloc(&s->dprobe_off, sizeof(long long) * nprobes));
+    NWB_CU(cudaMalloc(&s->dprobe_w, sizeof(double) * N3 * static_cast<size_t>(nprobes)));
+    NWB_CU(cudaMalloc(&s->dprobe_out, sizeof(double) * 6 * nprobes));
+    NWB_CU(cudaMemcpy(s->dprobe_off, node_offset, sizeof(long long) * nprobes, cudaMemcpyHostToDevice));
+    NWB_CU(cudaMemcpy(s->dprobe_w, weights, sizeof(double) * N3 * static_cast<size_t>(nprobes),
+                      cudaMemcpyHostToDevice));
+    s->nprobes = nprobes;
+    return NWB_OK;
+}
+
+nwb_status nwb_probe_read(nwb_solver* s, double* out) {
+    if (!s || !out) return fail(NWB_EINVAL, "nwb_probe_read: null argument");
+    if (s->nprobes == 0) return fail(NWB_EINVAL, "nwb_probe_read: no probes set up");
+    cudaError_t e = nwb::launch_probes(s->u[s->cur], s->stride, s->N * s->N * s->N, s->dprobe_off,
+                                       s->dprobe_w, s->nprobes, s->dprobe_out, s->st);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "probe kernel: %s", cudaGetErrorString(e));
+    ++s->launches;
+    NWB_CU(cudaMemcpyAsync(out, s->dprobe_out, sizeof(double) * 6 * s->nprobes, cudaMemcpyDeviceToHost,
+                           s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
+nwb_status nwb_snapshot_begin(nwb_solver* s, double* host, size_t n) {
+    if (!s || !host) return fail(NWB_EINVAL, "nwb_snapshot_begin: null argument");
+    if (n != 6 * static_cast<size_t>(s->npts))
+        return fail(NWB_EINVAL, "nwb_snapshot_begin: size %zu, expected 6*npts = %lld", n, 6 * s->npts);
+    if (!s->dsnap) {
+        NWB_CU(cudaStreamSynchronize(s->st));
+        NWB_CU(cudaMalloc(&s->dsnap, sizeof(double) * 6 * static_cast<size_t>(s->stride)));
+        NWB_CU(cudaStreamCreateWithFlags(&s->snap_st, cudaStreamNonBlocking));
+        NWB_CU(cudaEventCreateWithFlags(&s->snap_ev, cudaEventDisableTiming));
+    }
+    if (s->snap_pending) NWB_CU(cudaStreamSynchronize(s->snap_st));  // one snapshot in flight
+    // device copy in stream order (after every step queued so far), then the host
+    // copy on the snapshot stream, overlapping the steps queued after this call
+    NWB_CU(cudaMemcpyAsync(s->dsnap, s->u[s->cur], sizeof(double) * 6 * s->stride,
+                           cudaMemcpyDeviceToDevice, s->st));
+    NWB_CU(cudaEventRecord(s->snap_ev, s->st));
+    NWB_CU(cudaStreamWaitEvent(s->snap_st, s->snap_ev, 0));
+    NWB_CU(cudaMemcpy2DAsync(host, sizeof(double) * s->npts, s->dsnap, sizeof(double) * s->stride,
+                             sizeof(double) * s->npts, 6, cudaMemcpyDeviceToHost, s->snap_st));
+    s->snap_pending = true;
+    return NWB_OK;
+}
+
+nwb_status nwb_snapshot_wait(nwb_solver* s) {
+    if (!s) return fail(NWB_EINVAL, "nwb_snapshot_wait: null solver");
+    if (s->snap_pending) NWB_CU(cudaStreamSynchronize(s->snap_st));
+    s->snap_pending = false;
+    return NWB_OK;
+}
+
 nwb_status nwb_solver_destroy(nwb_solver* s) {
     if (!s) return NWB_OK;
     cudaStreamSynchronize(s->st);
+    if (s->snap_st) cudaStreamSynchronize(s->snap_st);
     s->release();
     delete s;
     return NWB_OK;

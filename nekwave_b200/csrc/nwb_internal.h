@@ -120,5 +120,8 @@ int energy_blocks(int nelt);
 
 // Large buffer write that evicts L2 (benchmark hygiene).
 cudaError_t launch_l2_flush(void* buf, size_t bytes, cudaStream_t st);
+// Probe values [nprobes][Ex..Hz] of state u (diag_kernels.cu).
+cudaError_t launch_probes(const double* u, long long stride, int N3, const long long* offset,
+                          const double* w, int nprobes, double* out, cudaStream_t st);
 
 }  // namespace nwb

@@ -121,6 +121,36 @@ class DgSolver:
         check(_lib.lib().nwb_energy(h, C.byref(e)))
         return e.value
 
+    def probeSetup(self, node_offset, weights) -> None:
+        """Probes as ProbeManager holds them (src/probe.cpp:33-96): per probe the first
+        node of its element (e*N^3) and its N^3 Lagrange weights."""
+        off = np.ascontiguousarray(node_offset, dtype=np.int64).reshape(-1)
+        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+        if w.size != off.size * self.info()["N"] ** 3:
+            raise ValueError("weights must hold N^3 values per probe")
+        check(_lib.lib().nwb_probe_setup(self._need(), off.size,
+                                         off.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                         w.ctypes.data_as(_lib._D)))
+        self._nprobes = off.size
+
+    def probeRead(self) -> np.ndarray:
+        """ProbeManager::record on the device: [nprobes, 6] (Ex, Ey, Ez, Hx, Hy, Hz)."""
+        out = np.empty(6 * getattr(self, "_nprobes", 0))
+        check(_lib.lib().nwb_probe_read(self._need(), out.ctypes.data_as(_lib._D)))
+        return out.reshape(-1, 6)
+
+    def snapshotBegin(self, host: np.ndarray) -> None:
+        """Start an asynchronous copy of the current state into host (6*npts doubles,
+        C-contiguous; pinned memory lets it overlap later steps)."""
+        if host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
+            raise ValueError("host must be a C-contiguous float64 array")
+        self._snap = host  # keep it alive until the copy lands
+        check(_lib.lib().nwb_snapshot_begin(self._need(), host.ctypes.data_as(_lib._D), host.size))
+
+    def snapshotWait(self) -> None:
+        check(_lib.lib().nwb_snapshot_wait(self._need()))
+        self._snap = None
+
     def info(self) -> dict:
         h = self._need()
         i = SolverInfo()

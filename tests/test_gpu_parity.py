@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from nekwave_b200 import DgSolver
+from nekwave_b200 import DgSolver, Mesh
 from oracle import oracle as O
 from tests.gpu_helpers import random_state, rel_l2, rel_max, smooth_state, solver_for
 
@@ -304,4 +304,60 @@ def test_structured_box_is_recognised(gpu, per):
     b = DgSolver("fp64")
     b.initializeBox(6, (4, 3, 2), (0, 0, 0), (1, 1, 1), 1.0, periodic=per)
     assert b.info()["structured"] == (4, 3, 2)
+    b.finalize()
+
+
+def test_probes_equal_the_reference_record_bit_for_bit(gpu):
+    """nwb_probe_read = ProbeManager::record: the same weights and node order, the
+    same multiply-then-add roundings, on the state after a few steps."""
+    from nekwave_b200.pool import locate_probes
+    N, nel = 6, (3, 2, 2)
+    mesh = Mesh(N)
+    mesh.createBoxMesh(*nel, 0.0, 1.5, 0.0, 1.0, 0.0, 1.0, False, False, False)
+    s = DgSolver()
+    s.initialize(mesh, 1.0)
+    u0 = random_state(O.box_mesh(N, nel, (0, 0, 0), (1.5, 1, 1)), 12)
+    s.uploadState(u0)
+    s.steps(0.5 * mesh.computeMinNodeDistance(), 3)
+    pts = [(0.1, 0.2, 0.3), (1.4, 0.9, 0.95), (0.75, 0.5, 0.5), (0.5, 0.5, 0.0)]
+    elems, w1d = locate_probes(mesh, pts)
+    w1d = w1d.reshape(len(pts), 3, N)
+    # ProbeManager's full weights: w[i + N(j + N k)] = wr[i] ws[j] wt[k]
+    wfull = np.einsum("pk,pj,pi->pkji", w1d[:, 2], w1d[:, 1], w1d[:, 0]).reshape(len(pts), -1)
+    off = elems.astype(np.int64) * N ** 3
+    s.probeSetup(off, wfull)
+    got = s.probeRead()
+    u = s.downloadState()
+    npts = u.size // 6
+    want = np.zeros((len(pts), 6))
+    for p in range(len(pts)):
+        for c in range(6):
+            acc = 0.0
+            for q in range(N ** 3):
+                acc = acc + wfull[p, q] * u[c * npts + off[p] + q]
+            want[p, c] = acc
+    np.testing.assert_array_equal(got, want)
+    s.finalize()
+
+
+def test_snapshot_while_stepping_equals_a_synchronous_download(gpu):
+    m = O.box_mesh(8, (6, 6, 6), (0, 0, 0), (1, 1, 1), (True, True, True))
+    u0 = smooth_state(m, 3)
+    dt = 0.5 * O.dxmin(m)
+    a = solver_for(m, 0.0)
+    a.uploadState(u0)
+    a.steps(dt, 7)
+    want = a.downloadState()
+    a.finalize()
+    b = solver_for(m, 0.0)
+    b.uploadState(u0)
+    host = np.empty(6 * m.npts)
+    b.steps(dt, 7)
+    b.snapshotBegin(host)
+    b.steps(dt, 20)            # keeps stepping while the copy is in flight
+    b.snapshotWait()
+    np.testing.assert_array_equal(host, want)
+    b.snapshotBegin(host)      # a second snapshot after the 20 further steps
+    b.snapshotWait()
+    np.testing.assert_array_equal(host, b.downloadState())
     b.finalize()
