@@ -159,6 +159,50 @@ __device__ __forceinline__ void add_lifts(const double* Fl, int c0, int i, int j
     }
 }
 
+// Numerical flux of one face point.  On an axis-aligned element (GEO_BOX) the
+// normal of face f lies along the axis of its reference direction (x for faces 1
+// and 3, y for 0 and 2, z for 4 and 5).  When its other two components are exactly
+// zero, n = s e_d, n x v = s (e_d x v) and n x (n x v) = -(v without its d
+// component), so the flux of src/device/dg_kernels.cu:264-294 reduces to eight
+// products (the normal components of both fields are zero); otherwise, and for
+// the other classes, the general form.  Used where a warp's face points never
+// span two faces (N^2 a multiple of 32): elsewhere the three branches diverge
+// within a warp and cost more than they save.
+template <typename TC, int GEO, int N>
+__device__ __forceinline__ void face_flux(int f, double nxd, double nyd, double nzd, double c0,
+                                          const double* jmp, TC* fl) {
+    if constexpr (GEO == GEO_BOX && (N * N) % 32 == 0) {
+        const TC dEx = static_cast<TC>(jmp[0]), dEy = static_cast<TC>(jmp[1]), dEz = static_cast<TC>(jmp[2]);
+        const TC dHx = static_cast<TC>(jmp[3]), dHy = static_cast<TC>(jmp[4]), dHz = static_cast<TC>(jmp[5]);
+        const TC hc0 = static_cast<TC>(0.5 * c0);
+        if ((f == 1 || f == 3) && nyd == 0.0 && nzd == 0.0) {
+            const TC hs = static_cast<TC>(0.5 * nxd);
+            fl[0] = TC(0); fl[3] = TC(0);
+            fl[1] = hc0 * dEy - hs * dHz; fl[2] = hs * dHy + hc0 * dEz;
+            fl[4] = hs * dEz + hc0 * dHy; fl[5] = hc0 * dHz - hs * dEy;
+            return;
+        }
+        if ((f == 0 || f == 2) && nxd == 0.0 && nzd == 0.0) {
+            const TC hs = static_cast<TC>(0.5 * nyd);
+            fl[1] = TC(0); fl[4] = TC(0);
+            fl[0] = hs * dHz + hc0 * dEx; fl[2] = hc0 * dEz - hs * dHx;
+            fl[3] = hc0 * dHx - hs * dEz; fl[5] = hs * dEx + hc0 * dHz;
+            return;
+        }
+        if ((f == 4 || f == 5) && nxd == 0.0 && nyd == 0.0) {
+            const TC hs = static_cast<TC>(0.5 * nzd);
+            fl[2] = TC(0); fl[5] = TC(0);
+            fl[0] = hc0 * dEx - hs * dHy; fl[1] = hs * dHx + hc0 * dEy;
+            fl[3] = hs * dEy + hc0 * dHx; fl[4] = hc0 * dHy - hs * dEx;
+            return;
+        }
+    }
+    numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
+                       static_cast<TC>(0.5 * c0), static_cast<TC>(jmp[0]), static_cast<TC>(jmp[1]),
+                       static_cast<TC>(jmp[2]), static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
+                       static_cast<TC>(jmp[5]), fl);
+}
+
 // Neighbour element across face f of element e of a structured box mesh
 // (x-fastest element order, faces 0..5 = y-, x+, y+, x-, z-, z+), -1 where the
 // face lies on a non-periodic wall; the matching face is the opposite one with
@@ -325,11 +369,7 @@ __device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, 
                 jmp[3] = G.nb[q][3] - Hxm; jmp[4] = G.nb[q][4] - Hym; jmp[5] = G.nb[q][5] - Hzm;
             }
             TC fl[6];
-            numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
-                               static_cast<TC>(0.5 * P.c0), static_cast<TC>(jmp[0]),
-                               static_cast<TC>(jmp[1]), static_cast<TC>(jmp[2]),
-                               static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
-                               static_cast<TC>(jmp[5]), fl);
+            face_flux<TC, GEO, N>(f, nxd, nyd, nzd, P.c0, jmp, fl);
             double* F = sflux + (team * 6 + f) * 6 * N2 + pq;
 #pragma unroll
             for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
@@ -397,11 +437,7 @@ __device__ __forceinline__ void face_phase_global(const StageParams& P, const in
             for (int c = 0; c < 6; ++c) jmp[c] = G.nb[q][c] - own[q][c];
         }
         TC fl[6];
-        numerical_flux<TC>(static_cast<TC>(nxd), static_cast<TC>(nyd), static_cast<TC>(nzd),
-                           static_cast<TC>(0.5 * P.c0), static_cast<TC>(jmp[0]),
-                           static_cast<TC>(jmp[1]), static_cast<TC>(jmp[2]),
-                           static_cast<TC>(jmp[3]), static_cast<TC>(jmp[4]),
-                           static_cast<TC>(jmp[5]), fl);
+        face_flux<TC, GEO, N>(f, nxd, nyd, nzd, P.c0, jmp, fl);
         double* F = sflux + (team * 6 + f) * 6 * N2 + pq;
 #pragma unroll
         for (int c = 0; c < 6; ++c) F[c * N2] = lift * static_cast<double>(fl[c]);
