@@ -361,3 +361,23 @@ def test_snapshot_while_stepping_equals_a_synchronous_download(gpu):
     b.snapshotWait()
     np.testing.assert_array_equal(host, b.downloadState())
     b.finalize()
+
+
+def test_nonfinite_state_is_reported_not_hidden(gpu):
+    """A NaN in the state: nwb_energy returns NWB_ENONFINITE (with the energy), the
+    context stays usable and a finite state afterwards is fine again."""
+    from nekwave_b200._lib import NwbError
+    m = O.box_mesh(4, (2, 2, 2), (0, 0, 0), (1, 1, 1))
+    s = solver_for(m, 1.0)
+    u = random_state(m, 2)
+    bad = u.copy()
+    bad[17] = np.nan
+    s.uploadState(bad)
+    s.steps(0.5 * O.dxmin(m), 2)
+    with pytest.raises(NwbError, match="NWB_ENONFINITE"):
+        s.energy()
+    s.uploadState(u)
+    assert abs(s.energy() - O.energy(m, u)) <= 1e-13 * O.energy(m, u)
+    with pytest.raises(NwbError, match="NWB_EINVAL"):
+        s.uploadState(u[:-6])
+    s.finalize()

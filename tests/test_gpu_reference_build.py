@@ -98,3 +98,31 @@ def test_reference_cuda_step_time(gpu, name, N, nel, lo, hi, per, c0):
         json.dump({"workload": name, "N": N, "nel": list(nel), "ms_per_step": ms / 10,
                    "gdof_stage_per_s": rate}, f)
     assert rate > 0
+
+
+def test_reference_cuda_serial_on_batch_instances(gpu):
+    """The reference's own DgSolver (its sm_100a build) solving the first 16 of the
+    256 batched cavities one at a time, as it would serve them: GDOF-stage/s over
+    the steps (CUDA events, mesh set-up excluded), recorded next to the pool's
+    (gpurun_out/ref_batch_serial.json)."""
+    from nekwave_b200.workloads import batch_instances
+    L = O.ref_gpu()
+    work = 0.0
+    ms_total = 0.0
+    steps = 40
+    for c in batch_instances(256, seed=0, steps=steps)[:16]:
+        mh = L.nwref_mesh_box(c.N, *c.nel, c.lo[0], c.hi[0], c.lo[1], c.hi[1], c.lo[2], c.hi[2], 0, 0, 0)
+        s = L.nwref_gpu_create(mh, c.c0)
+        u = np.zeros(6 * c.npts)
+        L.nwref_gpu_upload(s, O._dp(u), u.size)
+        L.nwref_gpu_steps(s, c.dt, 2)
+        ms_total += L.nwref_gpu_steps(s, c.dt, steps)
+        work += 6 * c.npts * 5 * steps
+        L.nwref_gpu_destroy(s)
+        L.nwref_mesh_free(mh)
+    rate = work / (ms_total / 1e3) / 1e9
+    os.makedirs(OUT, exist_ok=True)
+    with open(os.path.join(OUT, "ref_batch_serial.json"), "w") as f:
+        json.dump({"instances": 16, "steps_each": steps, "gdof_stage_per_s": rate,
+                   "ms_total": ms_total}, f)
+    assert rate > 0
