@@ -29,7 +29,7 @@ constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
 constexpr int count_simt() {
     int n = 0;
-    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1 && kShapes[i].alg != 100;
+    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1 && kShapes[i].alg != 200;
     return n;
 }
 constexpr int kNumSimt = count_simt();  // every variant but the FP64-only tensor-core ones (last)
@@ -45,19 +45,20 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                     return launch_mma8<v.minb>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
-            } else if constexpr (v.alg == 100) {
+            } else if constexpr (v.alg == 200) {
                 if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
                     return launch_dmma8<v.minb>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
-            } else if constexpr (v.alg >= 2 && v.alg <= 65) {
+            } else if constexpr (v.alg >= 2 && v.alg <= 129) {
                 static_assert(v.ksm == 0, "second family: k from L2");
                 constexpr int fl = v.alg - 2;
                 // the constant-bank D is an FP64 form; FP32-bulk runs the same shape without it
                 constexpr bool cd = (fl & 8) != 0 && !F32;
                 if constexpr (GEO == GEO_BOX || I == 0)
                     return launch2<NWB_N, GEO, F32, v.ks, v.epb, v.minb, (fl & 1) != 0, (fl & 2) != 0,
-                                   (fl & 4) != 0, cd, (fl & 16) != 0, (fl & 32) != 0>(p, st, cfg);
+                                   (fl & 4) != 0, cd, (fl & 16) != 0, (fl & 32) != 0,
+                                   (fl & 64) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == 0) {

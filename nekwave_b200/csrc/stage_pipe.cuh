@@ -28,6 +28,10 @@
 //          neighbour traces, connections, normals and lifts through the read-only
 //          path) while the tile's copies are in flight; the column phase follows
 //          the wait.  The face phase's latency then overlaps the tile's.
+//   DSMEM  (with SPLIT) the D rows a thread contracts with are read from shared
+//          memory at each use instead of being held in 2N registers, which buys
+//          resident blocks for the latency-bound orders at the price of more
+//          shared loads.
 //   EARLY  (without PIPE) the neighbour traces of the tile's face points are
 //          requested from global memory right after the tile's copies are issued,
 //          before the block waits for them, so both latencies overlap.  On a
@@ -445,7 +449,7 @@ __device__ __forceinline__ void face_phase_global(const StageParams& P, const in
 }
 
 template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
-          bool EARLY = false, bool FACEDONE = false>
+          bool EARLY = false, bool FACEDONE = false, bool DSMEM = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
@@ -545,7 +549,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 TC Vz_r = 0, Vy_r = 0, Vz_s = 0, Vx_s = 0, Vy_t = 0, Vx_t = 0;
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
-                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dr = DSMEM ? static_cast<TC>(sD[i + l * N]) : Dr[l];
+                    const TC ds = DSMEM ? static_cast<TC>(sD[j + l * N]) : Ds[l];
                     const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
@@ -561,7 +566,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 TC dr_[3] = {0, 0, 0}, ds_[3] = {0, 0, 0}, dt_[3] = {0, 0, 0};
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
-                    const TC dr = Dr[l], ds = Ds[l];
+                    const TC dr = DSMEM ? static_cast<TC>(sD[i + l * N]) : Dr[l];
+                    const TC ds = DSMEM ? static_cast<TC>(sD[j + l * N]) : Ds[l];
                     const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
@@ -695,7 +701,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
 }
 
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD, bool EARLY, bool FACEFIRST>
+          bool CONSTD, bool EARLY, bool FACEFIRST, bool DSMEM>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage2_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -720,7 +726,7 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
         else if constexpr (EARLY) gather2<N, GEO, KS, EPB, PAD, false>(P, t * EPB, nullptr, nullptr, tid, G);
         cp_async_wait<0>();
         __syncthreads();
-        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY, FACEFIRST>(
+        compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, EARLY, FACEFIRST, DSMEM>(
             P, t * EPB, su(0), sg(0), sc(0), sD, sflux, smem + L::uc, tid, G, P.Dc);
     } else {
         for (int n = 0; t < ntiles; ++n, t += gridDim.x) {
@@ -730,8 +736,8 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
             const int tn = t + gridDim.x;
             if (tn < ntiles) issue2<N, GEO, EPB, NT, PAD>(P, tn * EPB, su(b ^ 1), sg(b ^ 1), sc(b ^ 1), tid);
             cp_async_commit();
-            compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD>(P, t * EPB, su(b), sg(b), sc(b), sD, sflux,
-                                                               smem + L::uc, tid, G, P.Dc);
+            compute2<N, GEO, F32, KS, EPB, SPLIT, PAD, CONSTD, false, false, DSMEM>(
+                P, t * EPB, su(b), sg(b), sc(b), sD, sflux, smem + L::uc, tid, G, P.Dc);
         }
         cp_async_wait<0>();
     }
@@ -741,11 +747,11 @@ __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
 // at once (queried with the occupancy calculator on the first call, which the
 // solver makes at creation, outside any stream capture), never more than tiles.
 template <int N, int GEO, bool F32, int KS, int EPB, int MINB, bool PIPE, bool SPLIT, bool PAD,
-          bool CONSTD, bool EARLY, bool FACEFIRST>
+          bool CONSTD, bool EARLY, bool FACEFIRST, bool DSMEM>
 cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int threads = EPB * KS * N * N;
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
-    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY, FACEFIRST>;
+    auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY, FACEFIRST, DSMEM>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
     static int resident = 0;
     if (resident == 0) {
