@@ -1,13 +1,17 @@
 """Benchmark of the fused DG-SEM Maxwell LSRK45 path (libnwb) on B200.
 
-Workload (one GPU): periodic box [0,1]^3, 32x32x32 hexahedra, 8 GLL points per
-direction (order 7, 16.8 M nodes x 6 fields = 100.7 M DOF), central flux, CFL
-0.5, Gaussian pulse Ez = exp(-|r-r0|^2/sigma^2), sigma = 0.1, r0 ~ U[0.3,0.7]^3
-from the seed.  A "step" is one LSRK45 time step (five fused stage launches).
+Default workload (one GPU): periodic box [0,1]^3, 32x32x32 hexahedra, 8 GLL
+points per direction (order 7, 16.8 M nodes x 6 fields = 100.7 M DOF), central
+flux, CFL 0.5, Gaussian pulse Ez = exp(-|r-r0|^2/sigma^2), sigma = 0.1,
+r0 ~ U[0.3,0.7]^3 from the seed.  A "step" is one LSRK45 time step (five fused
+stage launches).  Other workloads: --workload c3 (PEC cavity 64x64x32, 6 points,
+upwind), batch (256 uneven PEC cavities in one pool), serve (Poisson stream of
+cavity solves, latency percentiles).
 
 metric: GDOF-stage/s = 6 * npts * 5 * steps / seconds / 1e9.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+                  [--workload c2|c3|batch|serve] [--accuracy-steps S]
   python bench.py --impl reference ...   # the reference's own CPU implementation
 
 With --gpus N > 1 (under torchrun) every rank advances its own independent

@@ -2,7 +2,7 @@
 //
 // Same arithmetic as stage_tile (stage_kernel.cuh): per element the volume curl,
 // the numerical flux with its lift, and the LSRK45 update, each residual entry
-// formed once in a fixed order.  Three independent options change the schedule
+// formed once in a fixed order.  Independent options change the schedule
 // and the shared-memory traffic:
 //
 //   PIPE   the block stays resident and walks the tiles t = blockIdx.x,
