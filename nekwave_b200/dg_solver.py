@@ -133,6 +133,18 @@ class DgSolver:
                                          w.ctypes.data_as(_lib._D)))
         self._nprobes = off.size
 
+    def probesAt(self, mesh, points) -> None:
+        """Probes at physical points of a box mesh, located and weighted as
+        ProbeManager::init does (src/probe.cpp:33-96)."""
+        from .pool import locate_probes
+        pts = [tuple(p) for p in points]
+        elems, w1d = locate_probes(mesh, pts)
+        N = mesh.getN()
+        w1d = w1d.reshape(len(pts), 3, N)
+        # full tensor weights w[i + N (j + N k)] = wr[i] ws[j] wt[k]
+        wfull = np.einsum("pk,pj,pi->pkji", w1d[:, 2], w1d[:, 1], w1d[:, 0]).reshape(len(pts), -1)
+        self.probeSetup(elems.astype(np.int64) * N ** 3, wfull)
+
     def probeRead(self) -> np.ndarray:
         """ProbeManager::record on the device: [nprobes, 6] (Ex, Ey, Ez, Hx, Hy, Hz)."""
         out = np.empty(6 * getattr(self, "_nprobes", 0))

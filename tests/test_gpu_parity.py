@@ -327,6 +327,8 @@ def test_probes_equal_the_reference_record_bit_for_bit(gpu):
     off = elems.astype(np.int64) * N ** 3
     s.probeSetup(off, wfull)
     got = s.probeRead()
+    s.probesAt(mesh, pts)                 # the same set-up from the points alone
+    np.testing.assert_array_equal(s.probeRead(), got)
     u = s.downloadState()
     npts = u.size // 6
     want = np.zeros((len(pts), 6))
