@@ -218,7 +218,7 @@ cudaError_t launch_n_alg(int stage, const SlotDev* slots, const WorkItem* work, 
         ? SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total
         : stage::Layout2<N, F32, Sh::EPB, false, (((ALG - 2) & 4) != 0)>::total;
     auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB, ALG>;
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;

@@ -142,7 +142,7 @@ cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg
     constexpr int smem = DmmaLayout8::total;
     auto kern = stage_dmma8_kernel<MINB>;
     if (cfg) *cfg = StageConfig{1, 1, 64, smem, 0, MINB};
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;

@@ -27,6 +27,7 @@
 #pragma once
 #include "nwb_internal.h"
 
+#include <atomic>
 #include <type_traits>
 
 namespace nwb {
@@ -418,7 +419,7 @@ cudaError_t launch_cfg(const StageParams* p, cudaStream_t st, StageConfig* cfg) 
     constexpr int smem = SmemLayout<N, F32, EPB, KSMEM>::total;
     auto kern = stage_kernel<N, GEO, F32, KS, EPB, KSMEM, MINB>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, KSMEM ? 1 : 0, MINB};
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;

@@ -250,7 +250,7 @@ cudaError_t launch_mma8(const StageParams* p, cudaStream_t st, StageConfig* cfg)
     constexpr int smem = MmaLayout8::total;
     auto kern = stage_kernel_mma8<MINB>;
     if (cfg) *cfg = StageConfig{2, 1, 128, smem, 0, MINB};
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;

@@ -753,7 +753,7 @@ cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
     auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY, FACEFIRST, DSMEM>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
-    static int resident = 0;
+    static std::atomic<int> resident{0};  // per kernel, shared by every host thread
     if (resident == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
@@ -765,9 +765,10 @@ cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
         if (occ < 1) return cudaErrorInvalidConfiguration;
         resident = occ * sms;
     }
+    const int res = resident;
     if (!p) return cudaSuccess;
     const int tiles = (p->nelt + EPB - 1) / EPB;
-    const int blocks = PIPE ? (tiles < resident ? tiles : resident) : tiles;
+    const int blocks = PIPE ? (tiles < res ? tiles : res) : tiles;
     kern<<<blocks, threads, smem, st>>>(*p);
     return cudaGetLastError();
 }
