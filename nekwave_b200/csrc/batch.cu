@@ -10,6 +10,7 @@
 #include "batch.cuh"
 #include "stage_kernel.cuh"
 #include "stage_pipe.cuh"
+#include "stage_dmma.cuh"
 
 namespace nwb {
 namespace {
@@ -20,7 +21,9 @@ using stage::stage_tile;
 // Shape per N for the batch kernel's blocks (kBatchThreads = 128): KS threads
 // per column, EPB elements, ALG the kernel family -- the single-mesh default's
 // family and arithmetic for each N (stage_variants.h entry 0), in a shape that
-// fits, so a cavity in the pool evolves bit for bit as it does alone.
+// fits, so a cavity in the pool evolves bit for bit as it does alone.  N = 8 in
+// FP64 runs the field-split tensor-core tile (stage_dmma.cuh, 128 threads) as the
+// single-mesh default does; ALG below is its FP32-bulk shape.
 template <int N> struct BShape;
 template <> struct BShape<2> { static constexpr int KS = 2, EPB = 16, ALG = 0; };
 template <> struct BShape<3> { static constexpr int KS = 1, EPB = 14, ALG = 0; };
@@ -32,10 +35,15 @@ template <> struct BShape<8> { static constexpr int KS = 2, EPB = 1, ALG = 8; };
 template <> struct BShape<9> { static constexpr int KS = 1, EPB = 1, ALG = 4; };
 template <> struct BShape<10> { static constexpr int KS = 1, EPB = 1, ALG = 0; };
 
+// N = 8 in FP64: the single-mesh default is the field-split tensor-core tile
+template <int N, bool F32>
+__host__ __device__ constexpr bool dmma_tile() { return N == 8 && !F32; }
+
 template <int N, bool F32>
 constexpr int bsmem() {
     using B = BShape<N>;
-    if constexpr (B::ALG == 0) return SmemLayout<N, F32, B::EPB, false>::total;
+    if constexpr (dmma_tile<N, F32>()) return stage::DmmaLayout8::total;
+    else if constexpr (B::ALG == 0) return SmemLayout<N, F32, B::EPB, false>::total;
     else return stage::Layout2<N, F32, B::EPB, false, (((B::ALG - 2) & 4) != 0)>::total;
 }
 
@@ -71,7 +79,10 @@ template <int N, bool F32>
 __device__ __forceinline__ void run_tile(const StageParams& P, int e0, unsigned char* smem, int tid) {
     using B = BShape<N>;
     static_assert(B::KS * B::EPB * N * N <= kBatchThreads, "shape too large");
-    if constexpr (B::ALG == 0)
+    if constexpr (dmma_tile<N, F32>())
+        stage::dmma8_tile<2>(P, e0, smem, tid,
+                             reinterpret_cast<const double*>(smem + stage::DmmaLayout8::D));
+    else if constexpr (B::ALG == 0)
         stage_tile<N, GEO_BOX, F32, B::KS, B::EPB, false, false>(P, e0, smem, tid);
     else
         tile2<N, F32, B::KS, B::EPB, B::ALG>(P, e0, smem, tid);
@@ -194,8 +205,40 @@ batch_stage_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restri
         tile2<N, F32, KS, EPB, ALG>(P, w.e0, smem, threadIdx.x, dp.d);
 }
 
+// N = 8 in FP64, per-N mode: the single-mesh default's field-split tensor-core tile
+// (128 threads, one element per block), D from dp (CD) or from shared memory.
+template <int MINB, bool CD>
+__global__ void __launch_bounds__(128, MINB)
+batch_dmma8_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work, int stage,
+                   int dry, const __grid_constant__ DParam dp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WorkItem w = work[blockIdx.x];
+    const SlotDev& S = slots[w.slot];
+    if (!S.active) return;
+    const StageParams P = slot_params(S, stage, dry);
+    stage::dmma8_tile<2>(P, w.e0, smem, threadIdx.x,
+                         CD ? dp.d : reinterpret_cast<const double*>(smem + stage::DmmaLayout8::D));
+}
+
+template <bool CD>
+cudaError_t launch_dmma8_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
+                           const DParam& dp, cudaStream_t st) {
+    constexpr int smem = stage::DmmaLayout8::total;
+    auto kern = batch_dmma8_kernel<4, CD>;
+    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (ntiles <= 0) return cudaSuccess;
+    kern<<<ntiles, 128, smem, st>>>(slots, work, stage, dry, dp);
+    return cudaGetLastError();
+}
+
 // Per-N shapes of the per-N mode: the single-mesh defaults (stage_variants.h entry
 // 0), with the persistent form of N = 4 replaced by its one-tile-per-block form.
+// N = 8 in FP64 runs batch_dmma8_kernel instead (NShape<8> is its FP32-bulk shape).
 // An ALG with CONSTD runs without it for an N whose cavities do not all share the
 // pool's D for that N (same arithmetic, D from shared memory).
 template <int N> struct NShape;
@@ -236,6 +279,18 @@ cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int 
                      const double* Dh, cudaStream_t st, int* epb_out) {
     using Sh = NShape<N>;
     if (epb_out) *epb_out = Sh::EPB;
+    if constexpr (dmma_tile<N, F32>()) {
+        DParam dp{};
+        if (Dh) {
+            for (int x = 0; x < N * N; ++x) dp.d[x] = Dh[x];
+            return launch_dmma8_n<true>(stage, slots, work, ntiles, dry, dp, st);
+        }
+        if (ntiles <= 0) {  // set-up call: prepare both forms
+            cudaError_t e = launch_dmma8_n<true>(stage, slots, work, 0, dry, dp, st);
+            if (e != cudaSuccess) return e;
+        }
+        return launch_dmma8_n<false>(stage, slots, work, ntiles, dry, dp, st);
+    }
     constexpr bool cd_bit = Sh::ALG >= 2 && ((Sh::ALG - 2) & 8) != 0;
     constexpr bool has_cd = cd_bit && !F32;  // the constant-bank D is an FP64 form
     constexpr int ALG_PLAIN = cd_bit ? Sh::ALG - 8 : Sh::ALG;

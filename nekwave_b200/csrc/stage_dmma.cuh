@@ -10,7 +10,8 @@
 // fragment load per lane per k-step) and keeps D in two registers.  tcgen05 has no
 // FP64 kind; mma.sync .f64 is sm_100a's FP64 tensor-core instruction.
 //
-// Block = one element, 64 threads = 2 warps:
+// Block = one element, 64 threads = 2 warps (or 128 threads, two warps per field
+// taking four planes each):
 //   1. cp.async of u_in (16-byte copies), D, geometry, connections; k lines of the
 //      element into L2;
 //   2. face phase (face_phase2, one thread per face point, six per thread);
@@ -42,54 +43,18 @@ struct DmmaLayout8 {
     static constexpr int total = flux + 36 * 64 * 8;
 };
 
-template <int MINB>
-__global__ void __launch_bounds__(64, MINB) stage_dmma8_kernel(const StageParams P) {
+// Planes K0 .. K0+NK-1 of the column phase of one warp (field src -> dst).
+template <int K0, int NK>
+__device__ __forceinline__ void dmma8_planes(const StageParams& P, const double* su, const double* V,
+                                             const double* Fl, int g, int t, int dst, double sgn,
+                                             double d0, double d1, const double (&cx)[8][2],
+                                             const double (&cy)[8][2], double rx, double sy, double tz,
+                                             long long ebase, const double* __restrict__ Dc) {
     constexpr int N = 8, N3 = 512;
-    using L = DmmaLayout8;
-    extern __shared__ __align__(16) unsigned char smem[];
-    double* su = reinterpret_cast<double*>(smem + L::u);
-    ElemGeo* sg = reinterpret_cast<ElemGeo*>(smem + L::geo);
-    int* sc = reinterpret_cast<int*>(smem + L::conn);
-    double* sD = reinterpret_cast<double*>(smem + L::D);
-    double* sflux = reinterpret_cast<double*>(smem + L::flux);
-    const int e = blockIdx.x;
-    const int tid = threadIdx.x;
-
-    issue2<N, GEO_BOX, 1, 64, false>(P, e, su, sg, sc, tid);
-    cp_async8(sD + tid, P.D + tid);
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();
-
-    FaceGather<face_points_per_thread<N, 1>()> G;
-    face_phase2<N, GEO_BOX, false, 1, 1, false, false>(P, e, su, sg, sc, sflux, tid, G);
-    __syncthreads();
-
-    const int warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int src = warp == 0 ? 3 : 0;   // differentiated field
-    const int dst = 3 - src;             // residual components formed
-    const double sgn = warp == 0 ? 1.0 : -1.0;
-    const double* V = su + src * N3;
-    const double d0 = sD[g + 8 * t];        // D(q = g, l = t)
-    const double d1 = sD[g + 8 * (4 + t)];  // D(q = g, l = 4 + t)
-    // the lane's two node columns of Vx and Vy (t derivatives)
-    double cx[8][2], cy[8][2];
-#pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        const double2 a = *reinterpret_cast<const double2*>(V + 0 * N3 + 64 * l + 8 * g + 2 * t);
-        const double2 b = *reinterpret_cast<const double2*>(V + 1 * N3 + 64 * l + 8 * g + 2 * t);
-        cx[l][0] = a.x; cx[l][1] = a.y;
-        cy[l][0] = b.x; cy[l][1] = b.y;
-    }
-    const double rx = sg->met[0], sy = sg->met[4], tz = sg->met[8];
     const double A = P.a, B = P.b, DT = P.dt;
     const long long S = P.stride;
-    const long long ebase = static_cast<long long>(e) * N3;
-    const double* Fl = sflux;
-
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = K0; k < K0 + NK; ++k) {
         const int ms = 64 * k + 8 * g + 2 * t;  // first of the lane's two nodes
         double2 kold[3];
 #pragma unroll
@@ -107,11 +72,12 @@ __global__ void __launch_bounds__(64, MINB) stage_dmma8_kernel(const StageParams
         dmma_f64(zs0, zs1, d1, V[2 * N3 + 64 * k + 8 * (4 + t) + g]);
         dmma_f64(xs0, xs1, d0, V[0 * N3 + 64 * k + 8 * t + g]);
         dmma_f64(xs0, xs1, d1, V[0 * N3 + 64 * k + 8 * (4 + t) + g]);
-        // t: sums over the cached columns, D(k, l) from the parameter bank
+        // t: sums over the cached columns, D(k, l) from Dc (the parameter bank when the
+        // caller has it there, else shared memory: the same values either way)
         double yt0 = 0.0, yt1 = 0.0, xt0 = 0.0, xt1 = 0.0;
 #pragma unroll
         for (int l = 0; l < 8; ++l) {
-            const double dk = P.Dc[k + 8 * l];
+            const double dk = Dc[k + 8 * l];
             yt0 += dk * cy[l][0]; yt1 += dk * cy[l][1];
             xt0 += dk * cx[l][0]; xt1 += dk * cx[l][1];
         }
@@ -137,11 +103,77 @@ __global__ void __launch_bounds__(64, MINB) stage_dmma8_kernel(const StageParams
     }
 }
 
-template <int MINB>
+// One element: WPF warps per field, 1 (64 threads, each warp all 8 planes of its
+// field) or 2 (128 threads, each warp 4 planes; the face phase then has 3 points
+// per thread).  Dc: D (column-major) where the t contraction reads it -- the
+// kernel's parameter copy when the caller has one (constant-bank operands), else
+// the tile's shared copy at smem + DmmaLayout8::D (the same values either way).
+// All threads of the block call it; threads beyond 64*WPF take part in the
+// barriers only.
+template <int WPF>
+__device__ __forceinline__ void dmma8_tile(const StageParams& P, const int e, unsigned char* smem,
+                                           const int tid, const double* Dc) {
+    constexpr int N = 8, N3 = 512, NT = 64 * WPF;
+    static_assert(WPF == 1 || WPF == 2, "one or two warps per field");
+    using L = DmmaLayout8;
+    double* su = reinterpret_cast<double*>(smem + L::u);
+    ElemGeo* sg = reinterpret_cast<ElemGeo*>(smem + L::geo);
+    int* sc = reinterpret_cast<int*>(smem + L::conn);
+    double* sD = reinterpret_cast<double*>(smem + L::D);
+    double* sflux = reinterpret_cast<double*>(smem + L::flux);
+
+    if (tid < NT) {
+        issue2<N, GEO_BOX, 1, NT, false>(P, e, su, sg, sc, tid);
+        if (tid < 64) cp_async8(sD + tid, P.D + tid);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    FaceGather<face_points_per_thread<N, WPF>()> G;
+    face_phase2<N, GEO_BOX, false, WPF, 1, false, false>(P, e, su, sg, sc, sflux, tid, G);
+    __syncthreads();
+    if (tid >= NT) return;
+
+    const int warp = tid >> 5, lane = tid & 31;
+    const int field = warp / WPF, part = warp % WPF;
+    const int g = lane >> 2, t = lane & 3;
+    const int src = field == 0 ? 3 : 0;  // differentiated field
+    const int dst = 3 - src;             // residual components formed
+    const double sgn = field == 0 ? 1.0 : -1.0;
+    const double* V = su + src * N3;
+    const double d0 = sD[g + 8 * t];        // D(q = g, l = t)
+    const double d1 = sD[g + 8 * (4 + t)];  // D(q = g, l = 4 + t)
+    // the lane's two node columns of Vx and Vy (t derivatives)
+    double cx[8][2], cy[8][2];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const double2 a = *reinterpret_cast<const double2*>(V + 0 * N3 + 64 * l + 8 * g + 2 * t);
+        const double2 b = *reinterpret_cast<const double2*>(V + 1 * N3 + 64 * l + 8 * g + 2 * t);
+        cx[l][0] = a.x; cx[l][1] = a.y;
+        cy[l][0] = b.x; cy[l][1] = b.y;
+    }
+    const double rx = sg->met[0], sy = sg->met[4], tz = sg->met[8];
+    const long long ebase = static_cast<long long>(e) * N3;
+    if constexpr (WPF == 1) {
+        dmma8_planes<0, 8>(P, su, V, sflux, g, t, dst, sgn, d0, d1, cx, cy, rx, sy, tz, ebase, Dc);
+    } else {
+        if (part == 0) dmma8_planes<0, 4>(P, su, V, sflux, g, t, dst, sgn, d0, d1, cx, cy, rx, sy, tz, ebase, Dc);
+        else dmma8_planes<4, 4>(P, su, V, sflux, g, t, dst, sgn, d0, d1, cx, cy, rx, sy, tz, ebase, Dc);
+    }
+}
+
+template <int MINB, int WPF>
+__global__ void __launch_bounds__(64 * WPF, MINB) stage_dmma8_kernel(const __grid_constant__ StageParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    dmma8_tile<WPF>(P, blockIdx.x, smem, threadIdx.x, P.Dc);
+}
+
+template <int MINB, int WPF = 1>
 cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int smem = DmmaLayout8::total;
-    auto kern = stage_dmma8_kernel<MINB>;
-    if (cfg) *cfg = StageConfig{1, 1, 64, smem, 0, MINB};
+    auto kern = stage_dmma8_kernel<MINB, WPF>;
+    if (cfg) *cfg = StageConfig{WPF, 1, 64 * WPF, smem, 0, MINB};
     static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -149,7 +181,7 @@ cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg
         attr_set = true;
     }
     if (!p) return cudaSuccess;
-    kern<<<p->nelt, 64, smem, st>>>(*p);
+    kern<<<p->nelt, 64 * WPF, smem, st>>>(*p);
     return cudaGetLastError();
 }
 

@@ -27,14 +27,33 @@ struct Shape {
 constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 #undef NWB_X
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
+// FP64 tensor-core shapes: axis-aligned class, FP64 only
+constexpr bool fp64_only(int alg) { return alg == 1 || alg == 200 || alg == 201; }
 constexpr int count_simt() {
     int n = 0;
-    for (int i = 0; i < kNumShapes; ++i) n += kShapes[i].alg != 1 && kShapes[i].alg != 200;
+    for (int i = 0; i < kNumShapes; ++i) n += !fp64_only(kShapes[i].alg);
     return n;
 }
-constexpr int kNumSimt = count_simt();  // every variant but the FP64-only tensor-core ones (last)
+constexpr int kNumSimt = count_simt();  // every shape but the FP64-only ones
+// Shape index of variant v among the shapes that are not FP64-only.
+constexpr int nth_general(int v) {
+    int c = 0;
+    for (int i = 0; i < kNumShapes; ++i)
+        if (!fp64_only(kShapes[i].alg)) {
+            if (c == v) return i;
+            ++c;
+        }
+    return -1;
+}
+constexpr int kFirstGeneral = nth_general(0);
+// Variant numbers: the axis-aligned class in FP64 has every shape in list order;
+// the axis-aligned class in FP32-bulk has the shapes that are not FP64-only, in
+// order; the other classes have one variant, the first such shape.
+inline int shape_index(int geo, int f32, int variant) {
+    return (geo == GEO_BOX && !f32) ? variant : nth_general(variant);
+}
 
-// every variant for the axis-aligned class, variant 0 for the others
+// vid: shape index (shape_index)
 template <int GEO, bool F32, int I>
 cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     if constexpr (I < kNumShapes) {
@@ -45,9 +64,9 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                     return launch_mma8<v.minb>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
-            } else if constexpr (v.alg == 200) {
+            } else if constexpr (v.alg == 200 || v.alg == 201) {
                 if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
-                    return launch_dmma8<v.minb>(p, st, cfg);
+                    return launch_dmma8<v.minb, v.alg - 199>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (v.alg >= 2 && v.alg <= 129) {
@@ -55,13 +74,13 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                 constexpr int fl = v.alg - 2;
                 // the constant-bank D is an FP64 form; FP32-bulk runs the same shape without it
                 constexpr bool cd = (fl & 8) != 0 && !F32;
-                if constexpr (GEO == GEO_BOX || I == 0)
+                if constexpr (GEO == GEO_BOX || I == kFirstGeneral)
                     return launch2<NWB_N, GEO, F32, v.ks, v.epb, v.minb, (fl & 1) != 0, (fl & 2) != 0,
                                    (fl & 4) != 0, cd, (fl & 16) != 0, (fl & 32) != 0,
                                    (fl & 64) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
-            } else if constexpr (GEO == GEO_BOX || I == 0) {
+            } else if constexpr (GEO == GEO_BOX || I == kFirstGeneral) {
                 return launch_cfg<NWB_N, GEO, F32, v.ks, v.epb, (v.ksm != 0), v.minb>(p, st, cfg);
             } else {
                 return cudaErrorInvalidValue;
@@ -85,16 +104,19 @@ template <>
 cudaError_t launch_stage_n<NWB_N>(int geo, int f32, int variant, const StageParams* p,
                                   cudaStream_t st, StageConfig* cfg) {
     using namespace stage;
+    const int nv = geo == GEO_BOX ? count_variants<GEO_BOX>(f32) : 1;
+    if (variant < 0 || variant >= nv) return cudaErrorInvalidValue;
+    const int vid = shape_index(geo, f32, variant);
     switch (geo) {
         case GEO_BOX:
-            return f32 ? launch_variant<GEO_BOX, true, 0>(variant, p, st, cfg)
-                       : launch_variant<GEO_BOX, false, 0>(variant, p, st, cfg);
+            return f32 ? launch_variant<GEO_BOX, true, 0>(vid, p, st, cfg)
+                       : launch_variant<GEO_BOX, false, 0>(vid, p, st, cfg);
         case GEO_AFFINE:
-            return f32 ? launch_variant<GEO_AFFINE, true, 0>(variant, p, st, cfg)
-                       : launch_variant<GEO_AFFINE, false, 0>(variant, p, st, cfg);
+            return f32 ? launch_variant<GEO_AFFINE, true, 0>(vid, p, st, cfg)
+                       : launch_variant<GEO_AFFINE, false, 0>(vid, p, st, cfg);
         case GEO_NODAL:
-            return f32 ? launch_variant<GEO_NODAL, true, 0>(variant, p, st, cfg)
-                       : launch_variant<GEO_NODAL, false, 0>(variant, p, st, cfg);
+            return f32 ? launch_variant<GEO_NODAL, true, 0>(vid, p, st, cfg)
+                       : launch_variant<GEO_NODAL, false, 0>(vid, p, st, cfg);
         default:
             return cudaErrorInvalidValue;
     }
