@@ -491,7 +491,9 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     tr = profiled_traffic(N)
     traffic = None
-    if tr and tr.get("npts") and tr.get("precision", "fp64") == args.precision:
+    # the committed capture is of the default shape (variant 0) in one precision
+    if (tr and tr.get("npts") and tr.get("precision", "fp64") == args.precision
+            and solver.info()["variant"] == 0):
         traffic = tr["dram_bytes_per_launch"] * npts / tr["npts"]
 
     # ---- end to end through the public API, host buffers, copies inside the timed region --
