@@ -1,8 +1,22 @@
 """Shared helpers of the GPU parity tests (imported by test modules only)."""
+import json
+import os
+
 import numpy as np
 
 from nekwave_b200 import DgSolver, Mesh
 from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def record(name: str, data: dict) -> None:
+    """Write a measurement a GPU test takes (timings, parity figures) as JSON into
+    the directory NWB_TEST_OUT names (default: test_out/ at the repository root)."""
+    out = os.environ.get("NWB_TEST_OUT", os.path.join(ROOT, "test_out"))
+    os.makedirs(out, exist_ok=True)
+    with open(os.path.join(out, name), "w") as f:
+        json.dump(data, f, indent=1)
 
 
 def solver_for(m: "O.MeshArrays", c0: float, precision: str = "fp64") -> DgSolver:

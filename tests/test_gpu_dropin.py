@@ -8,6 +8,8 @@ import subprocess
 
 import pytest
 
+from tests.gpu_helpers import record
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DROPIN = os.path.join(ROOT, "build", "dropin")
 
@@ -58,7 +60,8 @@ def test_reference_cli_end_to_end_against_dropin(gpu, tmp_path):
     per-step download, host probes and energy.  The CLI has no way to choose an
     initial wave (the reference ignores wave_type in a case file), so the fields
     start at zero and the run times the full Case::simulate loop; the energy
-    histories must agree.  Wall times are recorded (gpurun_out/cli_e2e.json)."""
+    histories must agree.  Wall times are recorded (cli_e2e.json in the test output
+    directory)."""
     import time
     case = {"mesh": {"nelx": 32, "nely": 32, "nelz": 32, "xmin": 0.0, "xmax": 1.0, "ymin": 0.0,
                      "ymax": 1.0, "zmin": 0.0, "zmax": 1.0, "periodic": "all"},
@@ -82,8 +85,6 @@ def test_reference_cli_end_to_end_against_dropin(gpu, tmp_path):
     a, b = out["reference"]["energies"], out["dropin"]["energies"]
     assert len(a) == len(b) >= 5
     assert all(abs(x - y) <= 1e-10 * abs(x) for x, y in zip(a, b))
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "cli_e2e.json"), "w") as f:
-        json.dump({"case": "periodic 32^3, 8 points, central, 50 steps, Case::simulate",
-                   "reference_wall_s": out["reference"]["wall_s"],
-                   "dropin_wall_s": out["dropin"]["wall_s"]}, f)
+    record("cli_e2e.json", {"case": "periodic 32^3, 8 points, central, 50 steps, Case::simulate",
+                            "reference_wall_s": out["reference"]["wall_s"],
+                            "dropin_wall_s": out["dropin"]["wall_s"]})

@@ -6,20 +6,14 @@ FP64 tolerance: the reference lifts face fluxes with atomicAdd in arbitrary
 order, so it is not bit-reproducible itself; its run-to-run spread is measured
 here and the new path must agree with it to 1e-12 relative L2 (1e-10 after 200
 steps)."""
-import json
-import os
-import time
-
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.gpu_helpers import rel_l2, smooth_state, solver_for
+from tests.gpu_helpers import record, rel_l2, smooth_state, solver_for
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not O.ref_gpu_available(), reason="reference CUDA build absent")]
-
-OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out")
 
 
 def ref_gpu_run(N, nel, lo, hi, per, c0, u0, dt, nsteps):
@@ -53,9 +47,7 @@ def test_tm110_matches_reference_cuda_build(gpu):
     ours = s.downloadState()
     s.finalize()
     err = rel_l2(ours, ref_a)
-    os.makedirs(OUT, exist_ok=True)
-    with open(os.path.join(OUT, "ref_parity_tm110.json"), "w") as f:
-        json.dump({"ref_run_to_run_rel_l2": spread, "ours_vs_ref_rel_l2": err}, f)
+    record("ref_parity_tm110.json", {"ref_run_to_run_rel_l2": spread, "ours_vs_ref_rel_l2": err})
     assert err < 1e-10
 
 
@@ -80,7 +72,7 @@ def test_random_state_matches_reference_cuda_build(gpu, N, nel, per, c0):
 def test_reference_cuda_step_time(gpu, name, N, nel, lo, hi, per, c0):
     """Times the reference's own DgSolver::step (CUDA events around 10 steps after 3
     warm-up steps, no per-step download) on the benchmark workloads and records it
-    next to ours (gpurun_out/ref_gpu_timing_<name>.json)."""
+    next to ours (ref_gpu_timing_<name>.json in the test output directory)."""
     L = O.ref_gpu()
     mh = L.nwref_mesh_box(N, *nel, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], *per)
     s = L.nwref_gpu_create(mh, c0)
@@ -93,10 +85,8 @@ def test_reference_cuda_step_time(gpu, name, N, nel, lo, hi, per, c0):
     L.nwref_gpu_destroy(s)
     L.nwref_mesh_free(mh)
     rate = 6 * npts * 5 * 10 / (ms / 1e3) / 1e9
-    os.makedirs(OUT, exist_ok=True)
-    with open(os.path.join(OUT, f"ref_gpu_timing_{name}.json"), "w") as f:
-        json.dump({"workload": name, "N": N, "nel": list(nel), "ms_per_step": ms / 10,
-                   "gdof_stage_per_s": rate}, f)
+    record(f"ref_gpu_timing_{name}.json", {"workload": name, "N": N, "nel": list(nel),
+                                           "ms_per_step": ms / 10, "gdof_stage_per_s": rate})
     assert rate > 0
 
 
@@ -104,7 +94,7 @@ def test_reference_cuda_serial_on_batch_instances(gpu):
     """The reference's own DgSolver (its sm_100a build) solving the first 16 of the
     256 batched cavities one at a time, as it would serve them: GDOF-stage/s over
     the steps (CUDA events, mesh set-up excluded), recorded next to the pool's
-    (gpurun_out/ref_batch_serial.json)."""
+    (ref_batch_serial.json in the test output directory)."""
     from nekwave_b200.workloads import batch_instances
     L = O.ref_gpu()
     work = 0.0
@@ -121,8 +111,6 @@ def test_reference_cuda_serial_on_batch_instances(gpu):
         L.nwref_gpu_destroy(s)
         L.nwref_mesh_free(mh)
     rate = work / (ms_total / 1e3) / 1e9
-    os.makedirs(OUT, exist_ok=True)
-    with open(os.path.join(OUT, "ref_batch_serial.json"), "w") as f:
-        json.dump({"instances": 16, "steps_each": steps, "gdof_stage_per_s": rate,
-                   "ms_total": ms_total}, f)
+    record("ref_batch_serial.json", {"instances": 16, "steps_each": steps,
+                                     "gdof_stage_per_s": rate, "ms_total": ms_total})
     assert rate > 0
