@@ -247,9 +247,9 @@ template <> struct NShape<3> { static constexpr int KS = 1, EPB = 16, KSM = 0, M
 template <> struct NShape<4> { static constexpr int KS = 2, EPB = 4, KSM = 0, MINB = 4, ALG = 12; };
 template <> struct NShape<5> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 4, ALG = 4; };
 template <> struct NShape<6> { static constexpr int KS = 2, EPB = 2, KSM = 0, MINB = 3, ALG = 4; };
-template <> struct NShape<7> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 4; };
+template <> struct NShape<7> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 12; };
 template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 4, ALG = 12; };
-template <> struct NShape<9> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 4; };
+template <> struct NShape<9> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 12; };
 template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
 
 template <int N, bool F32, int ALG>

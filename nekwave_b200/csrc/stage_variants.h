@@ -25,7 +25,7 @@
 #define NWB_VARIANTS_4(X) X(2, 4, 0, 3, 13) X(2, 4, 0, 3, 5) X(1, 8, 0, 4, 0) X(2, 4, 1, 1, 0) X(2, 4, 0, 4, 0) X(4, 4, 0, 2, 0) X(2, 4, 0, 4, 4) X(2, 8, 0, 2, 4) X(2, 4, 0, 4, 12) X(2, 4, 0, 4, 20) X(2, 4, 0, 4, 28)
 #define NWB_VARIANTS_5(X) X(2, 2, 0, 5, 68) X(2, 2, 0, 4, 4) X(1, 4, 0, 4, 0) X(1, 4, 1, 1, 0) X(5, 2, 0, 2, 0) X(1, 8, 0, 2, 0) X(2, 4, 0, 2, 4) X(2, 2, 0, 4, 8) X(2, 2, 0, 4, 12) X(2, 2, 0, 5, 4) X(2, 2, 0, 4, 20)
 #define NWB_VARIANTS_6(X) X(2, 2, 0, 3, 4) X(2, 2, 0, 3, 0) X(2, 2, 1, 1, 0) X(3, 2, 0, 2, 0) X(6, 1, 0, 2, 0) X(2, 4, 0, 1, 0) X(6, 1, 0, 3, 3) X(2, 2, 0, 3, 8) X(2, 2, 0, 3, 5) X(2, 2, 0, 3, 9) X(2, 4, 0, 2, 4) X(2, 2, 0, 3, 12) X(2, 2, 0, 3, 16) X(2, 2, 0, 4, 4) X(2, 2, 0, 5, 4) X(2, 4, 0, 2, 12) X(2, 2, 0, 3, 20) X(2, 2, 0, 3, 28) X(2, 2, 0, 3, 36) X(2, 2, 0, 3, 44)
-#define NWB_VARIANTS_7(X) X(2, 1, 0, 4, 4) X(1, 2, 0, 3, 0) X(1, 2, 1, 1, 0) X(7, 1, 0, 2, 0) X(1, 4, 0, 1, 0) X(2, 2, 0, 3, 4) X(2, 2, 0, 3, 8) X(2, 1, 0, 4, 12) X(2, 1, 0, 5, 4) X(2, 1, 0, 6, 4) X(2, 1, 0, 4, 20)
+#define NWB_VARIANTS_7(X) X(2, 1, 0, 4, 12) X(2, 1, 0, 4, 4) X(1, 2, 0, 3, 0) X(1, 2, 1, 1, 0) X(7, 1, 0, 2, 0) X(1, 4, 0, 1, 0) X(2, 2, 0, 3, 4) X(2, 2, 0, 3, 8) X(2, 1, 0, 5, 4) X(2, 1, 0, 6, 4) X(2, 1, 0, 4, 20)
 #define NWB_VARIANTS_8(X) X(2, 1, 0, 4, 201) X(2, 1, 0, 4, 12) X(2, 1, 0, 4, 8) X(2, 1, 0, 4, 0) X(2, 1, 1, 1, 0) X(4, 1, 0, 2, 0) X(8, 1, 0, 1, 0) X(1, 2, 0, 2, 0) X(2, 2, 0, 2, 0) X(4, 1, 0, 2, 3) X(2, 1, 0, 4, 4) X(2, 1, 0, 3, 5) X(2, 1, 0, 3, 9) X(2, 1, 0, 4, 6) X(2, 1, 0, 4, 16) X(2, 1, 0, 4, 28) X(2, 1, 0, 4, 20) X(2, 1, 0, 4, 44) X(2, 1, 0, 4, 36) X(1, 1, 0, 5, 200) X(2, 1, 0, 3, 201) X(2, 1, 0, 3, 1)
-#define NWB_VARIANTS_9(X) X(2, 1, 0, 2, 4) X(3, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(9, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8) X(2, 1, 0, 2, 12) X(2, 1, 0, 3, 12)
+#define NWB_VARIANTS_9(X) X(2, 1, 0, 2, 12) X(2, 1, 0, 2, 4) X(3, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(9, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8) X(2, 1, 0, 3, 12)
 #define NWB_VARIANTS_10(X) X(2, 1, 0, 2, 0) X(1, 1, 1, 1, 0) X(1, 1, 0, 2, 0) X(5, 1, 0, 1, 0) X(2, 1, 0, 3, 4) X(2, 1, 0, 3, 8) X(2, 1, 0, 2, 4) X(2, 1, 0, 2, 12)
