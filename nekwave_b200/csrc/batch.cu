@@ -134,6 +134,7 @@ batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict
         P.nfp = 0;
         P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
         P.spmask = 0;
+        for (int x = 0; x < 10; ++x) P.zl[x] = S.zl[x];
         P.c0 = S.c0;
         P.a = dry ? 0.0 : c_rk4a[stage];
         P.b = dry ? 0.0 : c_rk4b[stage];
@@ -173,6 +174,7 @@ __device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, 
     P.nfp = 0;
     P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
     P.spmask = 0;
+    for (int x = 0; x < 10; ++x) P.zl[x] = S.zl[x];
     P.c0 = S.c0;
     P.a = dry ? 0.0 : c_rk4a[stage];
     P.b = dry ? 0.0 : c_rk4b[stage];

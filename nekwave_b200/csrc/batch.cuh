@@ -24,6 +24,7 @@ struct SlotDev {
     const double* probe_w;  // [nprobes][3][N] tensor-product Lagrange weights
     long long stride;
     double c0, dt;
+    double zl[10];          // line coordinates of D (nwb::line_coords)
     int N, nelt, ntiles, epb;
     int nprobes, energy_every;
     int nsteps;             // steps this cavity must take

@@ -90,6 +90,40 @@ void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<doub
         }
 }
 
+// z with D z = 1, z[0] = -1: least squares over all N rows for z[1..N-1] (normal
+// equations of the N x (N-1) system D[:, 1:] z[1:] = 1 + D[:, 0], rank N-1),
+// Gaussian elimination with partial pivoting.
+void line_coords(int N, const double* D, double* z) {
+    const int n = N - 1;
+    double M[9][10] = {};
+    for (int a = 0; a < n; ++a) {
+        for (int b = 0; b < n; ++b) {
+            double s = 0.0;
+            for (int i = 0; i < N; ++i) s += D[i + N * (a + 1)] * D[i + N * (b + 1)];
+            M[a][b] = s;
+        }
+        double r = 0.0;
+        for (int i = 0; i < N; ++i) r += D[i + N * (a + 1)] * (1.0 + D[i]);
+        M[a][n] = r;
+    }
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::abs(M[r][c]) > std::abs(M[piv][c])) piv = r;
+        for (int x = 0; x <= n; ++x) std::swap(M[c][x], M[piv][x]);
+        for (int r = c + 1; r < n; ++r) {
+            const double f = M[r][c] / M[c][c];
+            for (int x = c; x <= n; ++x) M[r][x] -= f * M[c][x];
+        }
+    }
+    for (int c = n - 1; c >= 0; --c) {
+        double s = M[c][n];
+        for (int x = c + 1; x < n; ++x) s -= M[c][x] * z[x + 1];
+        z[c + 1] = s / M[c][c];
+    }
+    z[0] = -1.0;
+}
+
 // Trilinear map of one element with the reference's operation order
 // (src/mesh.cpp:188-314): position, J and J^{-T} (rx,sx,tx,ry,sy,ty,rz,sz,tz)
 // at reference point (r,s,t).

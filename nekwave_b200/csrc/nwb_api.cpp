@@ -211,6 +211,7 @@ struct nwb_solver {
     int cur = 0;
     double* dD = nullptr;
     double hD[100] = {};
+    double hzl[10] = {};  // line coordinates of hD (nwb::line_coords)
     int snel[3] = {0, 0, 0};  // structured box mesh (x-fastest elements), 0 = not
     int spmask = 0;
     // probes (nwb_probe_setup): node offset and N^3 weights per probe, device values
@@ -266,6 +267,7 @@ struct nwb_solver {
         P.b = kRK4B[stage];
         P.dt = dt;
         for (int x = 0; x < N * N; ++x) P.Dc[x] = hD[x];
+        for (int x = 0; x < N; ++x) P.zl[x] = hzl[x];
         for (int d = 0; d < 3; ++d) P.snel[d] = snel[d];
         P.spmask = spmask;
         return P;
@@ -537,6 +539,7 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
          if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
     NWB_H2D(s->dD, D, sizeof(double) * N2);
     for (int x = 0; x < N2; ++x) s->hD[x] = D[x];
+    nwb::line_coords(N, s->hD, s->hzl);
     NWB_H2D(s->dw3, w3, sizeof(double) * N3);
     if (s->geo != nwb::GEO_NODAL) {
         NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(nelt), &tot));

@@ -55,6 +55,8 @@ struct StageParams {
     int spmask;             // structured box mesh: periodic axes (bit 0 x, 1 y, 2 z)
     double Dc[100];         // D again, by value: kernels that index it with constants
                             // read it as an operand from the parameter bank
+    double zl[10];          // line coordinates: D zl = 1, zl[0] = -1 (the GLL nodes for
+                            // a GLL D); FP32-bulk fits a linear function with them
 };
 
 // Launch configuration of one fused-stage-kernel variant.
@@ -86,6 +88,11 @@ nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A);
 
 // Box meshes without per-node arrays (box_mesh.cpp).
 void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<double>& D);
+// Line coordinates from the differentiation matrix alone: the z with D z = 1 and
+// z[0] = -1 (unique, as D maps exactly the constants to zero).  For a GLL D these
+// are the GLL nodes; the reference's DgSolver::initialize reads no nodes, so the
+// solver derives them.
+void line_coords(int N, const double* D, double* z);
 void trilinear_point(const double c[8][3], double r, double s, double t, double* X, double* J,
                      double met[9]);
 void box_geometry(int N, int nelx, int nely, int nelz, const double lo[3], const double hi[3],

@@ -403,6 +403,7 @@ nwb_status admit(nwb_pool* p, int N, int nelt, const double* D, const double* w3
     d.k = p->ptr<double>(h.ranges[2]);
     d.D = p->ptr<double>(h.ranges[3]);
     d.w3 = p->ptr<double>(h.ranges[4]);
+    nwb::line_coords(N, D, d.zl);
     d.geo = p->ptr<nwb::ElemGeo>(h.ranges[5]);
     d.conn = p->ptr<int>(h.ranges[6]);
     d.partial = p->ptr<double>(h.ranges[7]);

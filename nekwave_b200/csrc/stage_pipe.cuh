@@ -78,7 +78,10 @@ struct Layout2 {
     static constexpr int D = conn0 + NB * conn_b;
     static constexpr int flux = D + align16(N2 * 8);
     static constexpr int uc = flux + EPB * 36 * N2 * 8;
-    static constexpr int total = uc + (F32 ? align16(6 * CS * 4) : 0);
+    // FP32-bulk: the tile's deviations [6][CS] floats, then per element the linear
+    // fit ([6][4]: centre value, slopes along r, s, t) and its curl ([6]), then zl
+    static constexpr int LIN = 30;
+    static constexpr int total = uc + (F32 ? align16(6 * CS * 4) + align16((EPB * LIN + 10) * 8) : 0);
     static_assert(tile % 16 == 0 && geo_b % 16 == 0, "16-byte aligned buffers");
 };
 
@@ -479,7 +482,10 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     const long long S = P.stride;
 
     const TC* s_uc;
-    if constexpr (F32) {
+    // FP32-bulk, affine classes: per element the linear fit's curl, added in FP64
+    constexpr int LIN = 30;
+    const double* s_lin = nullptr;
+    if constexpr (F32 && GEO == GEO_NODAL) {
         // FP32 copy of the tile as deviations from the element's centre node: the
         // derivatives are unchanged (rows of D sum to zero) and the rounding error
         // scales with the variation across the element instead of |u|
@@ -493,6 +499,61 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 w[c * CS + x] = static_cast<float>(su[c * CS + x] - ref);
             }
         s_uc = w;
+    } else if constexpr (F32) {
+        // FP32 copy of the tile as deviations w = u - L from a linear function L of
+        // the line coordinates zl, one per element and component (centre value and
+        // the slopes between opposite faces through the centre lines).  D zl = 1, so
+        // grad u = grad_FP32(w) + grad L, and on an affine element curl L is one
+        // constant per residual component, formed here in FP64 and added to the
+        // residual.  The FP32 rounding then scales with the departure from linear
+        // across the element instead of with the variation.
+        TC* w = reinterpret_cast<TC*>(smem_uc);
+        constexpr int lin_off = (6 * CS * 4 + 15) & ~15;  // after the deviations (Layout2::uc)
+        double* lin = reinterpret_cast<double*>(smem_uc + lin_off);
+        double* szl = lin + EPB * LIN;
+        constexpr int ic = N / 2;
+        const double inv = 1.0 / (P.zl[N - 1] - P.zl[0]);
+        const int nlin = tid < NT ? nvalid * 6 : 0;
+        if (tid == 0) {
+            // constant indices: a runtime index would move a caller's local P into
+            // local memory
+#pragma unroll
+            for (int x = 0; x < N; ++x) szl[x] = P.zl[x];
+        }
+        // (a) centre value and slopes of each component
+        for (int x = tid; x < nlin; x += NT) {
+            const int el = x / 6, c = x - 6 * el;
+            const double* U = su + c * CS + el * EN3;
+            double* Lc = lin + el * LIN + 4 * c;
+            Lc[0] = U[ic + RP * ic + PP * ic];
+            Lc[1] = (U[(N - 1) + RP * ic + PP * ic] - U[RP * ic + PP * ic]) * inv;
+            Lc[2] = (U[ic + RP * (N - 1) + PP * ic] - U[ic + PP * ic]) * inv;
+            Lc[3] = (U[ic + RP * ic + PP * (N - 1)] - U[ic + RP * ic]) * inv;
+        }
+        // (b) curl of L with the residual's sign: +curl H_L for E, -curl E_L for H
+        // (physical gradient = J^-T applied to the slopes; met = rx,sx,tx,ry,...,tz)
+        for (int x = tid; x < nlin; x += NT) {
+            const int el = x / 6, rc = x - 6 * el;
+            const int fld = rc / 3, q = rc - 3 * fld;
+            const int o = fld == 0 ? 3 : 0;  // the differentiated field
+            const double* m = sg[el].met;
+            double gr[3][3];                 // gr[comp][axis]
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double* U = su + (o + c) * CS + el * EN3;
+                const double ar = (U[(N - 1) + RP * ic + PP * ic] - U[RP * ic + PP * ic]) * inv;
+                const double as = (U[ic + RP * (N - 1) + PP * ic] - U[ic + PP * ic]) * inv;
+                const double at = (U[ic + RP * ic + PP * (N - 1)] - U[ic + RP * ic]) * inv;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) gr[c][d] = m[3 * d] * ar + m[3 * d + 1] * as + m[3 * d + 2] * at;
+            }
+            const double cx = gr[2][1] - gr[1][2], cy = gr[0][2] - gr[2][0], cz = gr[1][0] - gr[0][1];
+            const double cq = q == 0 ? cx : (q == 1 ? cy : cz);
+            lin[el * LIN + 24 + rc] = fld == 0 ? cq : -cq;
+        }
+        // (c), the deviations, follows the face phase's barrier
+        s_uc = w;
+        s_lin = lin;
     } else {
         s_uc = reinterpret_cast<const TC*>(su);
     }
@@ -500,6 +561,30 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     // ---- face phase (unless the caller ran it from global memory) -------------------
     if constexpr (!FACEDONE) face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY>(P, e0, su, sg, sc, sflux, tid, G);
     __syncthreads();
+
+    if constexpr (F32 && GEO != GEO_NODAL) {
+        // (c) FP32-bulk deviations w = u - L: each thread takes its own node column
+        // (i, j) of its element, planes h, h + KS, ... (the fit is complete: it was
+        // formed before the face phase's barrier)
+        if (active) {
+            TC* w = reinterpret_cast<TC*>(smem_uc);
+            const double* szl = s_lin + EPB * LIN;
+            constexpr int ic = N / 2;
+            const double zi = szl[i] - szl[ic], zj = szl[j] - szl[ic];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const double* Lc = s_lin + team * LIN + 4 * c;
+                const double base = Lc[0] + Lc[1] * zi + Lc[2] * zj;
+                const double at = Lc[3];
+                const int col = c * CS + team * EN3 + i + RP * j;
+                for (int k = h; k < N; k += KS) {
+                    const double Lv = base + at * (szl[k] - szl[ic]);
+                    w[col + PP * k] = static_cast<float>(su[col + PP * k] - Lv);
+                }
+            }
+        }
+        __syncthreads();
+    }
 
     // ---- column phase: volume curl + face terms + LSRK update ------------------
     if (!active) return;
@@ -615,6 +700,10 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 rhs[1] = sgn * static_cast<double>(c2);
                 rhs[2] = sgn * static_cast<double>(c3);
             }
+            if constexpr (F32 && GEO != GEO_NODAL) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) rhs[c] += s_lin[team * LIN + 24 + dst + c];
+            }
             add_lifts<N, 3>(Fl, dst, i, j, k, rhs);
             // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
 #pragma unroll
@@ -705,6 +794,10 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                     rhs[3 * fld + 1] = sg_ * static_cast<double>(c2);
                     rhs[3 * fld + 2] = sg_ * static_cast<double>(c3);
                 }
+            }
+            if constexpr (F32 && GEO != GEO_NODAL) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) rhs[c] += s_lin[team * LIN + 24 + c];
             }
             add_lifts<N, 6>(Fl, 0, i, j, k, rhs);
             // LSRK45 (src/device/dg_kernels.cu:404-406), FP64
