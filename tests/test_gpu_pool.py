@@ -199,3 +199,33 @@ def test_fp32_bulk_pool_error_vs_fp64(gpu):
     err = rel_l2(out["fp32"]["state"], out["fp64"]["state"])
     assert err < 1e-5, err
     assert np.all(np.abs(out["fp32"]["energy"] / out["fp64"]["energy"] - 1) < 1e-5)
+
+
+def test_fp32_bulk_smooth_pulse_within_1e6_and_pool_equals_single(gpu):
+    """The FP32-bulk class on a resolved smooth field (periodic box, 16^3 elements of
+    8 points, Gaussian Ez of width 3.2 element sizes, central flux, 500 steps): its
+    state stays within 1e-6 relative L2 of the FP64 path, and the pool evolves the
+    cavity bit for bit as the single-mesh FP32 solver does."""
+    N, nel, lo, hi, per, c0, ns = 8, (16, 16, 16), (0, 0, 0), (0.5, 0.5, 0.5), (True,) * 3, 0.0, 500
+    m = make_mesh(N, nel, lo, hi, per)
+    dt = 0.5 * m.computeMinNodeDistance()
+    x, y, z = m.getCoordX(), m.getCoordY(), m.getCoordZ()
+    n = m.getTotalPoints()
+    u0 = np.zeros(6 * n)
+    u0[2 * n:3 * n] = np.exp(-((x - 0.22) ** 2 + (y - 0.27) ** 2 + (z - 0.25) ** 2) / 0.1 ** 2)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        s = DgSolver(prec)
+        s.initialize(m, c0)
+        s.uploadState(u0)
+        s.steps(dt, ns)
+        out[prec] = s.downloadState()
+        s.finalize()
+    err = rel_l2(out["fp32"], out["fp64"])
+    assert err < 1e-6, err
+    pool = CavityPool(1 << 30, max_slots=2, precision="fp32")
+    s = pool.add(m, c0, dt, ns)
+    pool.upload(s, u0)
+    pool.step(ns)
+    np.testing.assert_array_equal(pool.results(s)["state"], out["fp32"])
+    pool.close()
