@@ -245,6 +245,26 @@ def test_every_launch_shape_matches_oracle(gpu, N, prec):
     s.finalize()
 
 
+@pytest.mark.parametrize("N", [5, 6, 8, 9])
+@pytest.mark.parametrize("nel", [(1, 1, 1), (2, 1, 1)])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_every_launch_shape_on_self_neighbour_meshes(gpu, N, nel, prec):
+    """Fully periodic meshes of one or two elements: across every face an element
+    meets itself or the other element of its tile, so the face phase takes its
+    neighbour traces from the resident tile, and tiles of several elements are
+    ragged (fewer valid elements than the shape holds)."""
+    m = O.box_mesh(N, nel, (0, 0, 0), (1, 1, 1), (True, True, True))
+    s = solver_for(m, 1.0, prec)
+    u = random_state(m, 5)
+    want = O.rhs(m, 1.0, u)
+    tol = RHS_TOL if prec == "fp64" else 1e-4
+    for v in range(s.info()["variant_count"]):
+        s.setVariant(v)
+        s.uploadState(u)
+        assert rel_max(s.evalRhs(), want) < tol, v
+    s.finalize()
+
+
 @pytest.mark.parametrize("N,nel", [(4, (24, 24, 24)), (5, (20, 16, 16)), (6, (16, 16, 16)),
                                    (7, (12, 12, 12)), (8, (16, 16, 12)), (9, (12, 12, 10))])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
