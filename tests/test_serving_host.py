@@ -1,0 +1,138 @@
+"""Admission logic of the serving loop (nekwave_b200/serving.py) on the CPU: the
+server runs against a stand-in for CavityPool that advances each resident cavity by
+the requested number of steps and charges each its three state arrays against the
+budget, so the policies can be checked without a GPU."""
+import numpy as np
+import pytest
+
+from nekwave_b200 import serving
+from nekwave_b200.pool import FINISHED, FREE, RUNNING
+from nekwave_b200.workloads import Cavity
+
+BYTES_PER_NODE = 3 * 6 * 8  # u[2] and k, six FP64 components
+
+
+class FakePool:
+    """The CavityPool calls the server makes, with a log of every admission."""
+
+    def __init__(self, budget, max_slots=512, precision="fp64"):
+        self.budget, self.max_slots = budget, max_slots
+        self.slots = {}     # slot -> [npts, nsteps, done]
+        self.log = []       # (request npts, nsteps, resident nodes after, cavities running before)
+        self.max_resident = 0
+
+    def resident(self):
+        return sum(v[0] for v in self.slots.values())
+
+    def add_box(self, N, nel, lo, hi, c0, dt, nsteps, periodic=(False,) * 3, probes=None,
+                energy_every=0):
+        npts = nel[0] * nel[1] * nel[2] * N ** 3
+        free = [s for s in range(self.max_slots) if s not in self.slots]
+        if not free or (self.resident() + npts) * BYTES_PER_NODE > self.budget:
+            raise serving.PoolFull("over budget")
+        running_before = len(self.slots)
+        self.slots[free[0]] = [npts, nsteps, 0]
+        self.log.append((npts, nsteps, self.resident(), running_before))
+        self.max_resident = max(self.max_resident, self.resident())
+        return free[0]
+
+    def init_pulse(self, slot, pulses):
+        assert slot in self.slots
+
+    def step(self, nsteps=1):
+        for v in self.slots.values():
+            v[2] = min(v[1], v[2] + nsteps)
+
+    def query(self):
+        status = np.full(self.max_slots, FREE, dtype=np.int32)
+        done = np.zeros(self.max_slots, dtype=np.int32)
+        for s, (_, nsteps, d) in self.slots.items():
+            status[s] = FINISHED if d >= nsteps else RUNNING
+            done[s] = d
+        return status, done
+
+    def results(self, slot, state=True, energy=True, probes=True):
+        nsteps = self.slots[slot][1]
+        return {"probes": np.zeros((nsteps + 1, 8, 6)), "energy": np.zeros(nsteps + 1)}
+
+    def remove(self, slot):
+        del self.slots[slot]
+
+    def close(self):
+        pass
+
+
+def requests(sizes):
+    """Cavities of (N, elements per direction, steps), arriving in list order."""
+    out = []
+    for i, (N, n, steps) in enumerate(sizes):
+        out.append(Cavity(N, (n, n, n), (0, 0, 0), (1, 1, 1), 1.0, steps, 1e-3,
+                          [(0.0, 0, 0, 0, 0.0)] * 6, arrival=1e-6 * i))
+    return out
+
+
+SIZES = [(8, 6, 40), (4, 2, 10), (9, 8, 30), (5, 3, 200), (6, 4, 5), (7, 5, 60), (4, 3, 100),
+         (8, 2, 7)]
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    made = []
+
+    def make(*a, **k):
+        made.append(FakePool(*a, **k))
+        return made[-1]
+
+    monkeypatch.setattr(serving, "CavityPool", make)
+    return made
+
+
+def run(policy, reqs, budget=1 << 40, saturation=1 << 40, chunk=4):
+    srv = serving.Server(budget, max_slots=16, precision="fp64", chunk=chunk, policy=policy,
+                         saturation_nodes=saturation)
+    results, _ = srv.run(reqs, time_scale=0.0)
+    srv.close()
+    return results
+
+
+@pytest.mark.parametrize("policy", ["fifo", "sjf"])
+def test_every_request_completes_with_its_histories(fake, policy):
+    reqs = requests(SIZES)
+    results = run(policy, reqs)
+    for i, r in enumerate(results):
+        assert r is not None and r.request == i
+        assert r.finished >= r.admitted >= 0.0 and r.latency >= 0.0
+        assert r.energy.shape == (reqs[i].nsteps + 1,) and r.probes.shape == (reqs[i].nsteps + 1, 8, 6)
+    assert not fake[0].slots  # every finished cavity was removed
+
+
+def test_fifo_admits_in_arrival_order(fake):
+    reqs = requests(SIZES)
+    run("fifo", reqs)
+    assert [(n, s) for n, s, _, _ in fake[0].log] == [(r.npts, r.nsteps) for r in reqs]
+
+
+def test_sjf_admits_shortest_work_first(fake):
+    reqs = requests(SIZES)
+    run("sjf", reqs)
+    order = sorted(reqs, key=lambda r: r.dof_stages)
+    assert [(n, s) for n, s, _, _ in fake[0].log] == [(r.npts, r.nsteps) for r in order]
+
+
+def test_sjf_keeps_resident_nodes_under_saturation(fake):
+    reqs = requests(SIZES)
+    sat = 300_000
+    results = run("sjf", reqs, saturation=sat)
+    assert all(r is not None for r in results)
+    for npts, _, resident, running_before in fake[0].log:
+        # over the limit only when it runs alone (a request larger than the limit)
+        assert resident <= sat or running_before == 0
+
+
+def test_full_pool_defers_admission(fake):
+    reqs = requests(SIZES)
+    largest = max(r.npts for r in reqs)
+    budget = (largest + 10_000) * BYTES_PER_NODE  # the largest cavity fits, with little room
+    results = run("fifo", reqs, budget=budget)
+    assert all(r is not None for r in results)
+    assert fake[0].max_resident * BYTES_PER_NODE <= budget
