@@ -37,7 +37,7 @@ def _worker(rank, world, port, out):
 
 def test_max_over_ranks_and_job_rate_with_two_gloo_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of this threaded process
         out = m.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
