@@ -42,30 +42,11 @@ BYTES_PER_DOF_STAGE = 32  # FP64 u and k, each read and written once
 
 
 def workload_spec(name, nel_override, seed):
-    """Single-mesh workloads: c2 (the headline) and c3 (PEC cavity 64x64x32, 6 points,
-    upwind, Gaussian Ex, Ey, Ez with independent seeded centres and widths)."""
-    r = np.random.Generator(np.random.PCG64(seed))
-    if name == "c3":
-        nel = (64, 64, 32) if nel_override == 32 else (2 * nel_override, 2 * nel_override, nel_override)
-        lo, hi = (0.0, 0.0, 0.0), (2.0, 2.0, 1.0)
-        pulses = []
-        for c in range(6):
-            if c < 3:
-                ctr = np.array(lo) + (np.array(hi) - np.array(lo)) * r.uniform(0.25, 0.75, 3)
-                pulses.append((1.0, ctr[0], ctr[1], ctr[2], float(r.uniform(0.05, 0.15))))
-            else:
-                pulses.append((0.0, 0, 0, 0, 0.0))
-        return dict(workload="pec_cavity_64x64x32_N6_upwind" if nel_override == 32 else
-                    f"pec_cavity_{nel[0]}x{nel[1]}x{nel[2]}_N6_upwind", N=6, nel=nel, lo=lo, hi=hi,
-                    periodic=(False, False, False), c0=1.0, flux="upwind", pulses=pulses)
-    nel = (nel_override,) * 3
-    r0 = r.uniform(0.3, 0.7, 3)
-    pulses = [(0.0, 0, 0, 0, 0.0)] * 2 + [(1.0, r0[0], r0[1], r0[2], WORKLOAD["sigma"])] + \
-        [(0.0, 0, 0, 0, 0.0)] * 3
-    return dict(workload=WORKLOAD["workload"] if nel_override == 32 else
-                f"periodic_box_{nel_override}^3_N8_central", N=8, nel=nel, lo=(0.0, 0.0, 0.0),
-                hi=(1.0, 1.0, 1.0), periodic=(True, True, True), c0=0.0, flux="central",
-                pulses=pulses)
+    """Single-mesh workloads c2 (the headline) and c3 (nekwave_b200.workloads)."""
+    from nekwave_b200.workloads import single_mesh
+    return single_mesh(name, nel_override, seed)
+
+
 L2_BYTES = 126 * 1024 * 1024
 
 

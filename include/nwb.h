@@ -65,7 +65,8 @@ typedef struct nwb_mesh_desc {
     const int* vol_idx_plus;      /* [nfp] FacePointData::volIdxPlus (-1: none)    */
     const int* bc_type;           /* [nfp] 0 interior/periodic, 1 PEC, 2 PMC       */
                                   /* (nonzero is a PEC mirror, as the reference's */
-                                  /* flux kernel does, src/device/dg_kernels.cu:244) */
+                                  /* flux kernel does, src/device/dg_kernels.cu:244; */
+                                  /* nwb_solver_create_ex can make 2 a PMC mirror) */
     const double* nx;             /* [nfp] outward unit normal                     */
     const double* ny;
     const double* nz;
@@ -113,6 +114,16 @@ void nwb_box_mesh_destroy(nwb_box_mesh* m);
  * The solver runs on the current CUDA device, on its own stream. */
 nwb_status nwb_solver_create(const nwb_mesh_desc* mesh, double c0,
                              nwb_precision precision, nwb_solver** out);
+/* nwb_solver_create with option flags (0: the same solver).  No counterpart in the
+ * reference, which mirrors PMC/SYM faces (bc_type 2) as PEC walls
+ * (src/dg_solver.cpp:92-98, src/device/dg_kernels.cu:243-251).
+ * NWB_SOLVER_TRUE_PMC: bc_type 2 face points become true PMC mirrors,
+ * [[E]] = 0 and [[H]] = -2 H^-, in the numerical flux; bc_type 1 and
+ * neighbourless points stay PEC mirrors.  Without it (the default, parity mode)
+ * the solver reproduces the reference. */
+#define NWB_SOLVER_TRUE_PMC 1u
+nwb_status nwb_solver_create_ex(const nwb_mesh_desc* mesh, double c0,
+                                nwb_precision precision, unsigned flags, nwb_solver** out);
 /* Solver on a box mesh built inside the library: the geometry of
  * Mesh::createBoxMesh (src/mesh.cpp:683-843) computed per element from the box
  * parameters, without per-node host arrays (large boxes need no host memory
@@ -140,6 +151,13 @@ nwb_status nwb_eval_rhs(nwb_solver* s, double* host_rhs, size_t n);
  * FP64, on the device (src/case.cpp:733-766).  Returns NWB_ENONFINITE (and the
  * non-finite energy) when the state holds NaN/Inf. */
 nwb_status nwb_energy(nwb_solver* s, double* energy);
+/* Largest |E| and |H| over the nodes of the current state, on the device:
+ * Case::getMaxE / Case::getMaxH (src/case.cpp:768-794), which the reference
+ * computes on the host from a full download every output step.  Same roundings
+ * as the host loop (no contraction, correctly rounded sqrt), so the values are
+ * equal bit for bit; NaN nodes are passed over as the host's comparison does.
+ * Synchronous; NWB_ENONFINITE when a maximum is infinite. */
+nwb_status nwb_max_norms(nwb_solver* s, double* max_e, double* max_h);
 /* Point probes on the device: ProbeManager::init's data (src/probe.cpp:33-96) --
  * per probe the first node of its element (e*N^3) and its N^3 tensor Lagrange
  * weights -- replace any earlier set; nprobes = 0 removes them. */
@@ -198,7 +216,9 @@ nwb_status nwb_solver_get_info(const nwb_solver* s, nwb_solver_info* info);
  * NWB_EINVAL.  The first call on a device looks up that array's device address
  * (once per device, with the device current); make that first call before any
  * stream capture.  All calls share the array: calls that overlap on the GPU race
- * and must be ordered by the caller. */
+ * and must be ordered by the caller.  Every pointer must be device (or managed)
+ * memory of the current device (nwb_set_device), and stream a stream of that
+ * device; a pointer of another device or of the host is refused with NWB_EINVAL. */
 #define NWB_ENERGY_NOALLOC_MAX_ELEMENTS 131072
 nwb_status nwb_energy_noalloc(const double* d_state, long long stride, int N, int nelt,
                               const double* d_jac, int jac_per_node, const double* d_w3,

@@ -23,6 +23,7 @@ NWB_ENOTFOUND = 7
 
 NWB_FP64 = 0
 NWB_FP32_BULK = 1
+NWB_SOLVER_TRUE_PMC = 1  # nwb_solver_create_ex flag
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
@@ -68,6 +69,8 @@ SIGNATURES = {
     "nwb_box_mesh_destroy": (None, [C.c_void_p]),
     "nwb_solver_create": (C.c_int, [C.POINTER(MeshDesc), C.c_double, C.c_int,
                                     C.POINTER(C.c_void_p)]),
+    "nwb_solver_create_ex": (C.c_int, [C.POINTER(MeshDesc), C.c_double, C.c_int, C.c_uint,
+                                       C.POINTER(C.c_void_p)]),
     "nwb_solver_create_box": (C.c_int, [C.c_int] * 4 + [C.c_double] * 6 +
                               [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
     "nwb_solver_init_pulse": (C.c_int, [C.c_void_p, _D]),
@@ -77,6 +80,7 @@ SIGNATURES = {
     "nwb_sync": (C.c_int, [C.c_void_p]),
     "nwb_eval_rhs": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_energy": (C.c_int, [C.c_void_p, _D]),
+    "nwb_max_norms": (C.c_int, [C.c_void_p, _D, _D]),
     "nwb_probe_setup": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), _D]),
     "nwb_probe_read": (C.c_int, [C.c_void_p, _D]),
     "nwb_snapshot_begin": (C.c_int, [C.c_void_p, _D, C.c_size_t]),

@@ -227,12 +227,8 @@ cudaError_t launch_dmma8_n(int stage, const SlotDev* slots, const WorkItem* work
                            const DParam& dp, cudaStream_t st) {
     constexpr int smem = stage::DmmaLayout8::total;
     auto kern = batch_dmma8_kernel<4, CD>;
-    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
     if (ntiles <= 0) return cudaSuccess;
     kern<<<ntiles, 128, smem, st>>>(slots, work, stage, dry, dp);
     return cudaGetLastError();
@@ -263,12 +259,8 @@ cudaError_t launch_n_alg(int stage, const SlotDev* slots, const WorkItem* work, 
         ? SmemLayout<N, F32, Sh::EPB, (Sh::KSM != 0)>::total
         : stage::Layout2<N, F32, Sh::EPB, false, (((ALG - 2) & 4) != 0)>::total;
     auto kern = batch_stage_n_kernel<N, F32, Sh::KS, Sh::EPB, (Sh::KSM != 0), Sh::MINB, ALG>;
-    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
     if (ntiles <= 0) return cudaSuccess;
     kern<<<ntiles, threads, smem, st>>>(slots, work, stage, dry, dp);
     return cudaGetLastError();

@@ -52,6 +52,60 @@ __global__ void energy_final_kernel(const double* __restrict__ partial, int n,
     }
 }
 
+// Largest |E| and |H| over the nodes of a contiguous range per block, as
+// Case::getMaxE / getMaxH (src/case.cpp:768-794) form them on the host:
+// sqrt((x*x + y*y) + z*z) with separate multiply, add and square-root roundings
+// (no contraction), kept when larger than the running maximum (a NaN node never
+// is).  The maximum does not depend on the order, so the result equals the
+// host's bit for bit.  partial[2b] = max|E|, partial[2b+1] = max|H| of block b.
+__device__ __forceinline__ double norm3_rn(double x, double y, double z) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+
+__global__ void __launch_bounds__(kEnergyThreads)
+maxnorm_partials_kernel(const double* __restrict__ u, long long stride, long long npts,
+                        double* __restrict__ partial) {
+    const long long per = (npts + gridDim.x - 1) / gridDim.x;
+    const long long lo = per * blockIdx.x;
+    const long long hi = min(npts, lo + per);
+    double me = 0.0, mh = 0.0;
+    for (long long p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+        const double e = norm3_rn(u[p], u[stride + p], u[2 * stride + p]);
+        const double h = norm3_rn(u[3 * stride + p], u[4 * stride + p], u[5 * stride + p]);
+        if (e > me) me = e;
+        if (h > mh) mh = h;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double oe = __shfl_down_sync(0xffffffffu, me, off);
+        const double oh = __shfl_down_sync(0xffffffffu, mh, off);
+        if (oe > me) me = oe;
+        if (oh > mh) mh = oh;
+    }
+    __shared__ double warp_max[2][kEnergyThreads / 32];
+    if ((threadIdx.x & 31) == 0) {
+        warp_max[0][threadIdx.x >> 5] = me;
+        warp_max[1][threadIdx.x >> 5] = mh;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double m = 0.0;
+        for (int w = 0; w < kEnergyThreads / 32; ++w)
+            if (warp_max[threadIdx.x][w] > m) m = warp_max[threadIdx.x][w];
+        partial[2 * blockIdx.x + threadIdx.x] = m;
+    }
+}
+
+__global__ void maxnorm_final_kernel(const double* __restrict__ partial, int n,
+                                     double* __restrict__ out) {
+    if (blockIdx.x == 0 && threadIdx.x < 2) {
+        double m = 0.0;
+        for (int b = 0; b < n; ++b)
+            if (partial[2 * b + threadIdx.x] > m) m = partial[2 * b + threadIdx.x];
+        out[threadIdx.x] = m;
+    }
+}
+
 // ProbeManager::record (src/probe.cpp:192-216): thread (probe, component) sums
 // w[p] * u[offset + p] over the probe element's N^3 nodes in node order, with
 // separate multiply and add roundings as on the host, so the values equal the
@@ -92,6 +146,15 @@ cudaError_t launch_energy(const double* u, long long stride, int N, int nelt,
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     energy_final_kernel<<<1, 32, 0, st>>>(partial, nblocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_norms(const double* u, long long stride, long long npts, double* partial,
+                             int nblocks, double* out, cudaStream_t st) {
+    maxnorm_partials_kernel<<<nblocks, kEnergyThreads, 0, st>>>(u, stride, npts, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    maxnorm_final_kernel<<<1, 32, 0, st>>>(partial, nblocks, out);
     return cudaGetLastError();
 }
 

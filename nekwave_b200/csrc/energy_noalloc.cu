@@ -127,6 +127,29 @@ extern "C" nwb_status nwb_energy_noalloc(const double* d_state, long long stride
     double* partials = nullptr;
     nwb_status st = scratch_address(&partials);
     if (st != NWB_OK) return st;
+    // every pointer must be device memory of the current device: the kernels run
+    // there, and the scratch address above is that device's
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        nwb_set_error_("nwb_energy_noalloc: no usable current CUDA device");
+        return NWB_ECUDA;
+    }
+    const void* ptrs[4] = {d_state, d_jac, d_w3, d_energy};
+    for (const void* q : ptrs) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();
+            nwb_set_error_("nwb_energy_noalloc: a pointer argument is not a CUDA pointer");
+            return NWB_EINVAL;
+        }
+        const bool on_dev = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+        if (!on_dev || a.device != dev) {
+            nwb_set_error_("nwb_energy_noalloc: every pointer must be device memory of the "
+                           "current device (nwb_set_device)");
+            return NWB_EINVAL;
+        }
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = (nelt + kWarpsPerBlock - 1) / kWarpsPerBlock;
     energy_element_kernel<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(

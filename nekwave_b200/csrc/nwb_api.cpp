@@ -88,7 +88,17 @@ nwb_status set_error(nwb_status s, const char* fmt, ...) {
     return s;
 }
 
-nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A) {
+// Wall code of face point fp: 0 (a neighbour), kConnPEC or kConnPMC.  The
+// reference mirrors PEC/W/V (bc 1), PMC/SYM/S (bc 2) and neighbourless points as
+// PEC alike (src/dg_solver.cpp:92-104, src/device/dg_kernels.cu:243-251); with
+// true_pmc, bc 2 points are PMC mirrors instead.
+int wall_code(const nwb_mesh_desc* m, long long fp, bool true_pmc) {
+    if (true_pmc && m->bc_type[fp] == 2) return nwb::kConnPMC;
+    if (m->bc_type[fp] != 0 || m->vol_idx_plus[fp] < 0) return nwb::kConnPEC;
+    return 0;
+}
+
+nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A, bool true_pmc) {
     const int N = m->N, nelt = m->nelt, N2 = N * N, N3 = N2 * N;
     const long long npts = static_cast<long long>(nelt) * N3;
     // canonical face-point order (src/mesh.cpp:1003-1004) is part of the contract
@@ -130,13 +140,13 @@ nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A) {
             if (std::abs(G.met[c]) > 1e-13 * scale) box = false;
         for (int f = 0; f < 6 && affine; ++f) {
             const long long fp0 = (static_cast<long long>(e) * 6 + f) * N2;
-            const bool pec0 = m->bc_type[fp0] != 0 || m->vol_idx_plus[fp0] < 0;
+            const int pec0 = wall_code(m, fp0, true_pmc);
             const double n0[3] = {m->nx[fp0], m->ny[fp0], m->nz[fp0]};
             const int vm0 = m->vol_idx_minus[fp0];
             const double lift0 = m->dA[fp0] / (m->jac[vm0] * m->w3[vm0 - base]);
             for (int pq = 0; pq < N2; ++pq) {
                 const long long fp = fp0 + pq;
-                const bool pec = m->bc_type[fp] != 0 || m->vol_idx_plus[fp] < 0;
+                const int pec = wall_code(m, fp, true_pmc);
                 const int vm = m->vol_idx_minus[fp];
                 const double lift = m->dA[fp] / (m->jac[vm] * m->w3[vm - base]);
                 if (pec != pec0 || std::abs(m->nx[fp] - n0[0]) > 1e-12 ||
@@ -150,7 +160,7 @@ nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A) {
             for (int c = 0; c < 3; ++c) G.nrm[f][c] = n0[c];
             G.lift[f] = lift0;
             if (pec0) {
-                A->conn[6 * static_cast<size_t>(e) + f] = nwb::kConnPEC;
+                A->conn[6 * static_cast<size_t>(e) + f] = pec0;
                 continue;
             }
             const int eB = m->vol_idx_plus[fp0] / N3;
@@ -367,7 +377,8 @@ struct nwb_solver {
 
 namespace {
 nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* D, const double* w3,
-                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out);
+                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out,
+                         bool true_pmc);
 }  // namespace
 
 extern "C" {
@@ -396,6 +407,11 @@ nwb_status nwb_set_device(int device) {
 }
 
 nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision prec, nwb_solver** out) {
+    return nwb_solver_create_ex(m, c0, prec, 0u, out);
+}
+
+nwb_status nwb_solver_create_ex(const nwb_mesh_desc* m, double c0, nwb_precision prec, unsigned flags,
+                                nwb_solver** out) {
     if (!out) return fail(NWB_EINVAL, "nwb_solver_create: out is null");
     *out = nullptr;
     if (!m) return fail(NWB_EINVAL, "nwb_solver_create: mesh is null");
@@ -413,15 +429,18 @@ nwb_status nwb_solver_create(const nwb_mesh_desc* m, double c0, nwb_precision pr
     const long long npts = static_cast<long long>(m->nelt) * N3;
     if (m->nelt > (1 << 25) || npts > 0x7fffffffLL)
         return fail(NWB_EINVAL, "nwb_solver_create: mesh too large for 32-bit node indices");
+    if (flags & ~static_cast<unsigned>(NWB_SOLVER_TRUE_PMC))
+        return fail(NWB_EINVAL, "nwb_solver_create_ex: unknown flags 0x%x", flags);
+    const bool true_pmc = (flags & NWB_SOLVER_TRUE_PMC) != 0;
 
     Analysis A;
     try {
-        nwb_status r = nwb::analyse_mesh(m, &A);
+        nwb_status r = nwb::analyse_mesh(m, &A, true_pmc);
         if (r != NWB_OK) return r;
     } catch (const std::bad_alloc&) {
         return fail(NWB_ENOMEM, "nwb_solver_create: out of host memory");
     }
-    return create_solver(m, N, m->nelt, m->D, m->w3, A, c0, prec, out);
+    return create_solver(m, N, m->nelt, m->D, m->w3, A, c0, prec, out, true_pmc);
 }
 
 }  // extern "C"
@@ -489,7 +508,8 @@ bool detect_structure(const std::vector<int>& conn, int nelt, int nel[3], int* p
 // Allocates and uploads a solver from analysed geometry.  m supplies the
 // per-node arrays of the general class and may be null for the affine classes.
 nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* D, const double* w3,
-                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out) {
+                         Analysis& A, double c0, nwb_precision prec, nwb_solver** out,
+                         bool true_pmc) {
     const int N2 = N * N, N3 = N2 * N;
     const long long npts = static_cast<long long>(nelt) * N3;
     nwb_solver* s = new (std::nothrow) nwb_solver();
@@ -532,8 +552,9 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
     NWB_TRY(dalloc(&s->k, 6 * static_cast<size_t>(s->stride), &tot));
     NWB_TRY(dalloc(&s->dD, static_cast<size_t>(N2), &tot));
     NWB_TRY(dalloc(&s->dw3, static_cast<size_t>(N3), &tot));
-    NWB_TRY(dalloc(&s->dpartial, static_cast<size_t>(s->eblocks), &tot));
-    NWB_TRY(dalloc(&s->denergy, 1, &tot));
+    // partial sums of the energy, or (max|E|, max|H|) pairs; energy, max|E|, max|H|
+    NWB_TRY(dalloc(&s->dpartial, 2 * static_cast<size_t>(s->eblocks), &tot));
+    NWB_TRY(dalloc(&s->denergy, 3, &tot));
 #define NWB_H2D(dst, src, bytes) \
     do { ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
          if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
@@ -556,12 +577,12 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
             std::vector<int> fpl(nfp);
             for (size_t fp = 0; fp < nfp; ++fp) {
                 const int vm = m->vol_idx_minus[fp];
-                const bool pec = m->bc_type[fp] != 0 || m->vol_idx_plus[fp] < 0;
+                const int wall = nwb::wall_code(m, static_cast<long long>(fp), true_pmc);
                 fn[fp] = m->nx[fp];
                 fn[nfp + fp] = m->ny[fp];
                 fn[2 * nfp + fp] = m->nz[fp];
                 fl[fp] = m->dA[fp] / (m->jac[vm] * m->w3[vm % N3]);
-                fpl[fp] = pec ? -1 : m->vol_idx_plus[fp];
+                fpl[fp] = wall ? wall : m->vol_idx_plus[fp];
             }
             NWB_TRY(dalloc(&s->dmet_n, 9 * static_cast<size_t>(s->stride), &tot));
             NWB_TRY(dalloc(&s->djac_n, static_cast<size_t>(npts), &tot));
@@ -630,7 +651,8 @@ nwb_status nwb_solver_create_box(int N, int nelx, int nely, int nelz, double xmi
             if (std::abs(A.egeo[e].met[c]) > 1e-13 * scale) box = false;
     }
     A.geo = box ? nwb::GEO_BOX : nwb::GEO_AFFINE;
-    nwb_status r = create_solver(nullptr, N, static_cast<int>(nelt), D.data(), w3.data(), A, c0, prec, out);
+    nwb_status r = create_solver(nullptr, N, static_cast<int>(nelt), D.data(), w3.data(), A, c0, prec, out,
+                                 false);
     if (r != NWB_OK) return r;
     nwb_solver* s = *out;
     s->box.lo[0] = xmin; s->box.lo[1] = ymin; s->box.lo[2] = zmin;
@@ -716,6 +738,22 @@ nwb_status nwb_energy(nwb_solver* s, double* out) {
     NWB_CU(cudaMemcpyAsync(out, s->denergy, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     NWB_CU(cudaStreamSynchronize(s->st));
     if (!std::isfinite(*out)) return fail(NWB_ENONFINITE, "nwb_energy: state holds NaN/Inf");
+    return NWB_OK;
+}
+
+nwb_status nwb_max_norms(nwb_solver* s, double* max_e, double* max_h) {
+    if (!s || !max_e || !max_h) return fail(NWB_EINVAL, "nwb_max_norms: null argument");
+    cudaError_t e = nwb::launch_max_norms(s->u[s->cur], s->stride, s->npts, s->dpartial, s->eblocks,
+                                          s->denergy + 1, s->st);
+    if (e != cudaSuccess) return fail(NWB_ECUDA, "max-norm kernel: %s", cudaGetErrorString(e));
+    s->launches += 2;
+    double h[2];
+    NWB_CU(cudaMemcpyAsync(h, s->denergy + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    *max_e = h[0];
+    *max_h = h[1];
+    if (!std::isfinite(h[0]) || !std::isfinite(h[1]))
+        return fail(NWB_ENONFINITE, "nwb_max_norms: state holds Inf");
     return NWB_OK;
 }
 

@@ -2,10 +2,36 @@
 // kernels (stage_kernels.cu, diag_kernels.cu).
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace nwb {
+
+// One-time kernel set-up per device.  cudaFuncSetAttribute (and the occupancy a
+// launcher derives from it) applies to the current device's context only, so a
+// launcher keeps one flag per device index: a process that creates solvers on
+// several GPUs sets each kernel up on each of them.
+constexpr int kMaxDeviceSlots = 64;
+inline cudaError_t current_device_slot(int* dev) {
+    cudaError_t e = cudaGetDevice(dev);
+    if (e != cudaSuccess) return e;
+    if (*dev < 0 || *dev >= kMaxDeviceSlots) return cudaErrorInvalidDevice;
+    return cudaSuccess;
+}
+// Raises kern's dynamic shared-memory limit to smem on the current device, once
+// per device (flags: one zero-initialised static array per kernel).
+template <typename K>
+cudaError_t set_smem_once(K kern, int smem, std::atomic<int>* flags) {
+    int dev = 0;
+    cudaError_t e = current_device_slot(&dev);
+    if (e != cudaSuccess) return e;
+    if (flags[dev].load(std::memory_order_acquire)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    flags[dev].store(1, std::memory_order_release);
+    return cudaSuccess;
+}
 
 // Geometry classes the mesh analysis sorts a mesh into (nwb_api.cpp).
 enum GeoKind : int {
@@ -28,11 +54,15 @@ struct alignas(16) ElemGeo {
 static_assert(sizeof(ElemGeo) == 272, "ElemGeo layout");
 
 // Face connection code of (element, face):
-//   -1                          PEC mirror ([[E]] = -2E^-, [[H]] = 0)
+//   -1                          PEC mirror ([[E]] = -2E^-, [[H]] = 0); the reference
+//                               applies it to PMC faces too (src/device/dg_kernels.cu:243-251)
+//   -2                          true PMC mirror ([[E]] = 0, [[H]] = -2H^-), only for
+//                               solvers created with NWB_SOLVER_TRUE_PMC
 //   (eB << 6) | (fB << 3) | o   neighbour element eB, its face fB, orientation o
 // Orientation o maps (p,q) on this face to (p',q') on the neighbour face:
 //   (a,b) = (o & 4) ? (q,p) : (p,q);  p' = (o & 1) ? N-1-a : a;  q' = (o & 2) ? N-1-b : b.
 constexpr int kConnPEC = -1;
+constexpr int kConnPMC = -2;
 
 struct StageParams {
     const double* u_in;     // [6][stride]
@@ -84,7 +114,9 @@ struct Analysis {
     std::vector<int> conn;
     std::vector<double> jac_e;
 };
-nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A);
+// true_pmc: bc_type 2 faces become kConnPMC (per-node class: neighbour -2) instead
+// of the reference's PEC mirror.
+nwb_status analyse_mesh(const nwb_mesh_desc* m, Analysis* A, bool true_pmc = false);
 
 // Box meshes without per-node arrays (box_mesh.cpp).
 void gll(int N, std::vector<double>& z, std::vector<double>& w, std::vector<double>& D);
@@ -124,6 +156,10 @@ cudaError_t launch_energy(const double* u, long long stride, int N, int nelt,
                           const double* jac_e, const double* jac_n, const double* w3,
                           double* partial, int nblocks, double* out, cudaStream_t st);
 int energy_blocks(int nelt);
+// Largest |E| and |H| over the nodes of u (diag_kernels.cu), out[0], out[1] on the
+// device; partial holds 2*nblocks doubles.
+cudaError_t launch_max_norms(const double* u, long long stride, long long npts, double* partial,
+                             int nblocks, double* out, cudaStream_t st);
 
 // Large buffer write that evicts L2 (benchmark hygiene).
 cudaError_t launch_l2_flush(void* buf, size_t bytes, cudaStream_t st);

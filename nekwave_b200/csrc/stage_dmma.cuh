@@ -174,12 +174,8 @@ cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg
     constexpr int smem = DmmaLayout8::total;
     auto kern = stage_dmma8_kernel<MINB, WPF>;
     if (cfg) *cfg = StageConfig{WPF, 1, 64 * WPF, smem, 0, MINB};
-    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
     if (!p) return cudaSuccess;
     kern<<<p->nelt, 64 * WPF, smem, st>>>(*p);
     return cudaGetLastError();

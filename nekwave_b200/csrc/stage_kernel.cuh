@@ -102,6 +102,21 @@ __device__ __forceinline__ void numerical_flux(T nx, T ny, T nz, T hc0, T dEx, T
     f[5] = -half * nxE_z - hc0 * nnH_z;
 }
 
+// Jumps at a wall face point (neighbour code < 0) from the own traces (E-, H-).
+// kConnPEC: the PEC mirror [[E]] = -2E-, [[H]] = 0 of src/device/dg_kernels.cu:243-251,
+// which the reference also applies to PMC faces.  kConnPMC (solvers created with
+// NWB_SOLVER_TRUE_PMC only): the PMC mirror [[E]] = 0, [[H]] = -2H-.
+__device__ __forceinline__ void wall_jumps(long long code, double Ex, double Ey, double Ez,
+                                           double Hx, double Hy, double Hz, double jmp[6]) {
+    if (code == kConnPMC) {
+        jmp[0] = 0.0; jmp[1] = 0.0; jmp[2] = 0.0;
+        jmp[3] = -2.0 * Hx; jmp[4] = -2.0 * Hy; jmp[5] = -2.0 * Hz;
+    } else {
+        jmp[0] = -2.0 * Ex; jmp[1] = -2.0 * Ey; jmp[2] = -2.0 * Ez;
+        jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+    }
+}
+
 // One tile (EPB consecutive elements starting at e0) of one stage.  Called by
 // all threads of a block; threads tid >= EPB*KS*N*N take part in the barriers
 // only (the batched kernel runs every N in blocks of one fixed size).
@@ -203,7 +218,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
             const int m = face_local<N>(f, p, q);
             const double Exm = U[0 * CS + m], Eym = U[1 * CS + m], Ezm = U[2 * CS + m];
             const double Hxm = U[3 * CS + m], Hym = U[4 * CS + m], Hzm = U[5 * CS + m];
-            long long vB = -1;  // neighbour node (global index), -1 = mirror
+            long long vB = kConnPEC;  // neighbour node (global index), < 0: a wall code
             double nxd, nyd, nzd, lift;
             if constexpr (GEO == GEO_NODAL) {
                 const long long g = (static_cast<long long>(e) * 6 + f) * N2 + pq;
@@ -214,7 +229,8 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
                 lift = P.flift[g];
             } else {
                 const int cd = s_conn[team * 6 + f];
-                if (cd != kConnPEC) {
+                vB = cd;
+                if (cd >= 0) {
                     const int eB = cd >> 6, fB = (cd >> 3) & 7, o = cd & 7;
                     int a = (o & 4) ? q : p;
                     int b = (o & 4) ? p : q;
@@ -230,9 +246,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& P, const int e0,
             }
             double jmp[6];
             if (vB < 0) {
-                // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
-                jmp[0] = -2.0 * Exm; jmp[1] = -2.0 * Eym; jmp[2] = -2.0 * Ezm;
-                jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+                wall_jumps(vB, Exm, Eym, Ezm, Hxm, Hym, Hzm, jmp);
             } else {
                 const long long eB = vB / N3;
                 double vals[6];
@@ -419,12 +433,8 @@ cudaError_t launch_cfg(const StageParams* p, cudaStream_t st, StageConfig* cfg) 
     constexpr int smem = SmemLayout<N, F32, EPB, KSMEM>::total;
     auto kern = stage_kernel<N, GEO, F32, KS, EPB, KSMEM, MINB>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, KSMEM ? 1 : 0, MINB};
-    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
     if (!p) return cudaSuccess;
     const int blocks = (p->nelt + EPB - 1) / EPB;
     kern<<<blocks, threads, smem, st>>>(*p);

@@ -105,11 +105,13 @@ __device__ __forceinline__ void stage_tile_mma8(const StageParams& P, const int 
     const int pq = tid & 63, p = pq & 7, q = pq >> 3;
     double nb[3][6];
     bool mirror[3];
+    int wall[3];  // wall code of a mirror face (kConnPEC or kConnPMC)
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const int f = d == 0 ? (side ? 1 : 3) : (d == 1 ? (side ? 2 : 0) : (side ? 5 : 4));
         const int cd = __ldg(P.conn + e * 6 + f);
-        mirror[d] = cd == kConnPEC;
+        mirror[d] = cd < 0;
+        wall[d] = cd;
         if (!mirror[d]) {
             const int eB = cd >> 6, fB = (cd >> 3) & 7, o = cd & 7;
             int a = (o & 4) ? q : p;
@@ -206,9 +208,7 @@ __device__ __forceinline__ void stage_tile_mma8(const StageParams& P, const int 
 #pragma unroll
         for (int c = 0; c < 6; ++c) own[c] = s_u[c * UE + mu];
         if (mirror[d]) {
-            // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
-            jmp[0] = -2.0 * own[0]; jmp[1] = -2.0 * own[1]; jmp[2] = -2.0 * own[2];
-            jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+            wall_jumps(wall[d], own[0], own[1], own[2], own[3], own[4], own[5], jmp);
         } else {
 #pragma unroll
             for (int c = 0; c < 6; ++c) jmp[c] = nb[d][c] - own[c];
@@ -250,12 +250,8 @@ cudaError_t launch_mma8(const StageParams* p, cudaStream_t st, StageConfig* cfg)
     constexpr int smem = MmaLayout8::total;
     auto kern = stage_kernel_mma8<MINB>;
     if (cfg) *cfg = StageConfig{2, 1, 128, smem, 0, MINB};
-    static std::atomic<bool> attr_set{false};  // per kernel, shared by every host thread
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
     if (!p) return cudaSuccess;
     kern<<<p->nelt, 128, smem, st>>>(*p);
     return cudaGetLastError();

@@ -229,7 +229,8 @@ __device__ __forceinline__ int struct_neighbour(const StageParams& P, int ex, in
 }
 
 // Neighbour values of the face points of one thread (FPT of them): the global
-// node vB across each point (-1: mirror) and its six field values.
+// node vB across each point (< 0: the wall code kConnPEC or kConnPMC) and its six
+// field values.
 template <int FPT>
 struct FaceGather {
     double nb[FPT][6];
@@ -263,7 +264,7 @@ __device__ __forceinline__ void gather2(const StageParams& P, const int e0, cons
 #pragma unroll
     for (int q = 0; q < FPT; ++q) {
         const int fp = lt + q * TPE;
-        long long vB = -1;
+        long long vB = kConnPEC;  // < 0: a wall code
         if (team < nvalid && fp < 6 * N2) {
             const int f = fp / N2;
             const int pq = fp - f * N2;
@@ -282,7 +283,8 @@ __device__ __forceinline__ void gather2(const StageParams& P, const int e0, cons
                 int cd;
                 if constexpr (FROM_SMEM) cd = sc[team * 6 + f];
                 else cd = __ldg(P.conn + e * 6 + f);
-                if (cd != kConnPEC) {
+                vB = cd;
+                if (cd >= 0) {
                     const int fB = (cd >> 3) & 7, o = cd & 7;
                     eB = cd >> 6;
                     int a = (o & 4) ? qq : p;
@@ -368,9 +370,7 @@ __device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, 
             }
             double jmp[6];
             if (G.vB[q] < 0) {
-                // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
-                jmp[0] = -2.0 * Exm; jmp[1] = -2.0 * Eym; jmp[2] = -2.0 * Ezm;
-                jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+                wall_jumps(G.vB[q], Exm, Eym, Ezm, Hxm, Hym, Hzm, jmp);
             } else {
                 jmp[0] = G.nb[q][0] - Exm; jmp[1] = G.nb[q][1] - Eym; jmp[2] = G.nb[q][2] - Ezm;
                 jmp[3] = G.nb[q][3] - Hxm; jmp[4] = G.nb[q][4] - Hym; jmp[5] = G.nb[q][5] - Hzm;
@@ -436,9 +436,7 @@ __device__ __forceinline__ void face_phase_global(const StageParams& P, const in
         }
         double jmp[6];
         if (G.vB[q] < 0) {
-            // PEC mirror: [[E]] = -2 E^-, [[H]] = 0 (src/device/dg_kernels.cu:244-251)
-            jmp[0] = -2.0 * own[q][0]; jmp[1] = -2.0 * own[q][1]; jmp[2] = -2.0 * own[q][2];
-            jmp[3] = 0.0; jmp[4] = 0.0; jmp[5] = 0.0;
+            wall_jumps(G.vB[q], own[q][0], own[q][1], own[q][2], own[q][3], own[q][4], own[q][5], jmp);
         } else {
 #pragma unroll
             for (int c = 0; c < 6; ++c) jmp[c] = G.nb[q][c] - own[q][c];
@@ -864,19 +862,21 @@ cudaError_t launch2(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int smem = Layout2<N, F32, EPB, PIPE, PAD>::total;
     auto kern = stage2_kernel<N, GEO, F32, KS, EPB, MINB, PIPE, SPLIT, PAD, CONSTD, EARLY, FACEFIRST, DSMEM>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, smem, 0, MINB};
-    static std::atomic<int> resident{0};  // per kernel, shared by every host thread
-    if (resident == 0) {
+    // resident blocks on the device, per kernel and device (0: not yet set up)
+    static std::atomic<int> resident[kMaxDeviceSlots];
+    int dev = 0;
+    if (cudaError_t e = current_device_slot(&dev); e != cudaSuccess) return e;
+    if (resident[dev].load(std::memory_order_acquire) == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        int dev = 0, sms = 0, occ = 0;
-        e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int sms = 0, occ = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
         if (e != cudaSuccess) return e;
         if (occ < 1) return cudaErrorInvalidConfiguration;
-        resident = occ * sms;
+        resident[dev].store(occ * sms, std::memory_order_release);
     }
-    const int res = resident;
+    const int res = resident[dev].load(std::memory_order_acquire);
     if (!p) return cudaSuccess;
     const int tiles = (p->nelt + EPB - 1) / EPB;
     const int blocks = PIPE ? (tiles < res ? tiles : res) : tiles;

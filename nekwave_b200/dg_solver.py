@@ -35,13 +35,16 @@ class DgSolver:
         self._h = None
         self._npts = 0
 
-    def initialize(self, mesh, c0: float) -> bool:
-        """Analyse the mesh and allocate the device state (DgSolver::initialize)."""
+    def initialize(self, mesh, c0: float, true_pmc: bool = False) -> bool:
+        """Analyse the mesh and allocate the device state (DgSolver::initialize).
+        true_pmc: PMC faces (bc 2) are PMC mirrors instead of the reference's PEC
+        mirror (nwb_solver_create_ex, NWB_SOLVER_TRUE_PMC)."""
         self.finalize()
         L = _lib.lib()
         h = C.c_void_p()
         d = mesh.desc()
-        check(L.nwb_solver_create(C.byref(d), float(c0), self._prec, C.byref(h)))
+        flags = _lib.NWB_SOLVER_TRUE_PMC if true_pmc else 0
+        check(L.nwb_solver_create_ex(C.byref(d), float(c0), self._prec, flags, C.byref(h)))
         self._h = h
         self._npts = mesh.getTotalPoints()
         self._mesh = mesh
@@ -120,6 +123,13 @@ class DgSolver:
         e = C.c_double()
         check(_lib.lib().nwb_energy(h, C.byref(e)))
         return e.value
+
+    def maxNorms(self):
+        """(max |E|, max |H|) over the nodes, on the device (Case::getMaxE/getMaxH,
+        src/case.cpp:768-794), equal to the host loop bit for bit."""
+        e, h = C.c_double(), C.c_double()
+        check(_lib.lib().nwb_max_norms(self._need(), C.byref(e), C.byref(h)))
+        return e.value, h.value
 
     def probeSetup(self, node_offset, weights) -> None:
         """Probes as ProbeManager holds them (src/probe.cpp:33-96): per probe the first

@@ -1,9 +1,9 @@
 """Seeded synthetic workloads of the benchmark configurations (no dataset exists
 for this path; every input is generated from a seed with numpy PCG64).
 
-  tm110_cube()        PEC unit cube, 4^3 elements, 5 points, TM110 mode
-  periodic_pulse()    periodic [0,1]^3, 32^3 elements, 8 points, Gaussian Ez
-  pec_cavity_pulse()  PEC [0,2]x[0,2]x[0,1], 64x64x32 elements, 6 points
+  single_mesh("c2")   periodic [0,1]^3, 32^3 elements, 8 points, central, Gaussian Ez
+  single_mesh("c3")   PEC [0,2]x[0,2]x[0,1], 64x64x32 elements, 6 points, upwind,
+                      Gaussians in Ex, Ey, Ez
   batch_instances()   256 PEC cavities, uneven sizes and orders
   serving_requests()  Poisson stream of cavity solves
 """
@@ -82,6 +82,48 @@ class Cavity:
         return 6 * self.npts * 5 * self.nsteps
 
 
+def single_mesh(name="c2", nel=32, seed=0) -> dict:
+    """Single-mesh workloads.  c2: periodic [0,1]^3, nel^3 elements (32: the
+    headline), 8 points, central flux, Ez = exp(-|r-r0|^2/0.1^2) with r0 ~
+    U[0.3,0.7]^3.  c3: PEC [0,2]x[0,2]x[0,1], 2nel x 2nel x nel elements (nel = 32:
+    64x64x32), 6 points, upwind, Gaussians in Ex, Ey, Ez with independent centres
+    in the middle half of each axis and sigma ~ U[0.05,0.15].  pulses[c] =
+    (amp, x0, y0, z0, sigma) per component, as nwb_solver_init_pulse takes them."""
+    r = rng(seed)
+    if name == "c3":
+        nel3 = (64, 64, 32) if nel == 32 else (2 * nel, 2 * nel, nel)
+        lo, hi = (0.0, 0.0, 0.0), (2.0, 2.0, 1.0)
+        pulses = []
+        for c in range(6):
+            if c < 3:
+                ctr = np.array(lo) + (np.array(hi) - np.array(lo)) * r.uniform(0.25, 0.75, 3)
+                pulses.append((1.0, ctr[0], ctr[1], ctr[2], float(r.uniform(0.05, 0.15))))
+            else:
+                pulses.append((0.0, 0, 0, 0, 0.0))
+        return dict(workload="pec_cavity_64x64x32_N6_upwind" if nel == 32 else
+                    f"pec_cavity_{nel3[0]}x{nel3[1]}x{nel3[2]}_N6_upwind", N=6, nel=nel3, lo=lo,
+                    hi=hi, periodic=(False, False, False), c0=1.0, flux="upwind", pulses=pulses)
+    if name != "c2":
+        raise ValueError(f"unknown single-mesh workload {name!r}")
+    r0 = r.uniform(0.3, 0.7, 3)
+    pulses = [(0.0, 0, 0, 0, 0.0)] * 2 + [(1.0, r0[0], r0[1], r0[2], 0.1)] + [(0.0, 0, 0, 0, 0.0)] * 3
+    return dict(workload="periodic_box_32x32x32_N8_central" if nel == 32 else
+                f"periodic_box_{nel}^3_N8_central", N=8, nel=(nel,) * 3, lo=(0.0, 0.0, 0.0),
+                hi=(1.0, 1.0, 1.0), periodic=(True, True, True), c0=0.0, flux="central",
+                pulses=pulses)
+
+
+def pulse_state(pulses, x, y, z):
+    """Host state of per-component Gaussian pulses on given node coordinates (the
+    function nwb_solver_init_pulse evaluates on the device)."""
+    n = x.size
+    u = np.zeros(6 * n)
+    for comp, (a, x0, y0, z0, s) in enumerate(pulses):
+        if s > 0:
+            u[comp * n:(comp + 1) * n] = a * np.exp(-((x - x0) ** 2 + (y - y0) ** 2 + (z - z0) ** 2) / s ** 2)
+    return u
+
+
 def _pulse_ez(r, lo, hi, sig):
     lo, hi = np.asarray(lo, float), np.asarray(hi, float)
     c = lo + (hi - lo) * r.uniform(0.25, 0.75, 3)
@@ -132,9 +174,4 @@ def serving_requests(n, rate, seed=0, max_nel=48, max_order=8):
 
 def cavity_state(c: Cavity, x, y, z):
     """Host initial state of a cavity on given node coordinates."""
-    n = x.size
-    u = np.zeros(6 * n)
-    for comp, (a, x0, y0, z0, s) in enumerate(c.pulses):
-        if s > 0:
-            u[comp * n:(comp + 1) * n] = a * np.exp(-((x - x0) ** 2 + (y - y0) ** 2 + (z - z0) ** 2) / s ** 2)
-    return u
+    return pulse_state(c.pulses, x, y, z)

@@ -444,6 +444,11 @@ static void volume_curl_elem(int N, int e, const double* D, const double* w3g,
     }
 }
 
+/* Off: the reference's behaviour (every bc != 0 point is a PEC mirror).  On: bc 2
+   points are PMC mirrors, the checker of libnwb's NWB_SOLVER_TRUE_PMC option. */
+static int g_true_pmc = 0;
+void nwo_set_true_pmc(int on) { g_true_pmc = on != 0; }
+
 void nwo_rhs(int N, int nelt, const double* D, const double* w3,
              const double* jac, const double* met,
              int nfp, const int* vmin, const int* vplus, const int* bc,
@@ -473,7 +478,12 @@ void nwo_rhs(int N, int nelt, const double* D, const double* w3,
         double Ex_m = u[0 * npts + vM], Ey_m = u[1 * npts + vM], Ez_m = u[2 * npts + vM];
         double Hx_m = u[3 * npts + vM], Hy_m = u[4 * npts + vM], Hz_m = u[5 * npts + vM];
         double dEx, dEy, dEz, dHx, dHy, dHz;
-        if (bc[p] || vplus[p] < 0) {
+        if (g_true_pmc && bc[p] == 2) {
+            /* option, not in the reference (which mirrors PMC faces as PEC):
+               PMC mirror [[E]] = 0, [[H]] = -2 H^- */
+            dEx = 0.0; dEy = 0.0; dEz = 0.0;
+            dHx = -2.0 * Hx_m; dHy = -2.0 * Hy_m; dHz = -2.0 * Hz_m;
+        } else if (bc[p] || vplus[p] < 0) {
             dEx = -2.0 * Ex_m; dEy = -2.0 * Ey_m; dEz = -2.0 * Ez_m;
             dHx = 0.0; dHy = 0.0; dHz = 0.0;
         } else {

@@ -73,6 +73,11 @@ void nwo_rhs(int N, int nelt, const double* D, const double* w3,
              const double* nx, const double* ny, const double* nz, const double* dA,
              double c0, const double* u, double* rhs);
 
+/* Off (default): bc != 0 points are PEC mirrors, as in the reference
+ * (src/device/dg_kernels.cu:243-251).  On: bc 2 points are PMC mirrors
+ * ([[E]] = 0, [[H]] = -2 H^-), the checker of libnwb's NWB_SOLVER_TRUE_PMC. */
+void nwo_set_true_pmc(int on);
+
 /* nsteps LSRK45 steps of size dt (src/dg_solver.cpp:306-527, coefficients :58-69,
  * update kernel src/device/dg_kernels.cu:393-408).  u and k (6*npts) are updated
  * in place; k must be zero before the first step (src/dg_solver.cpp:125). */

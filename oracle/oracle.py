@@ -64,6 +64,7 @@ def lib():
         L.nwo_energy.restype = C.c_double
         L.nwo_energy.argtypes = [C.c_int, C.c_int, _D, _D, _D]
         L.nwo_lsrk45.argtypes = [_D, _D]
+        L.nwo_set_true_pmc.argtypes = [C.c_int]
         L.nwo_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -124,6 +125,7 @@ def _bind_mesh_api(L):
     L.nwref_mesh_dxmin.restype = C.c_double
     L.nwref_mesh_dxmin.argtypes = [C.c_void_p]
     L.nwref_mesh_export.argtypes = [C.c_void_p] + [_D] * 9 + [_I] * 3 + [_D] * 4
+    L.nwref_mesh_coords.argtypes = [C.c_void_p, _D, _D, _D]
 
 
 @dataclass
@@ -274,18 +276,29 @@ def dxmin(m: MeshArrays) -> float:
     return lib().nwo_dxmin(m.N, m.nelt, _dp(m.x), _dp(m.y), _dp(m.zc))
 
 
-def rhs(m: MeshArrays, c0: float, u: np.ndarray) -> np.ndarray:
+def rhs(m: MeshArrays, c0: float, u: np.ndarray, true_pmc: bool = False) -> np.ndarray:
+    """true_pmc: bc 2 points are PMC mirrors (not the reference's behaviour, which
+    mirrors them as PEC; the checker of libnwb's NWB_SOLVER_TRUE_PMC)."""
     u = np.ascontiguousarray(u, dtype=np.float64)
     out = np.zeros(6 * m.npts)
-    lib().nwo_rhs(*m.geo_args(), float(c0), _dp(u), _dp(out))
+    lib().nwo_set_true_pmc(int(true_pmc))
+    try:
+        lib().nwo_rhs(*m.geo_args(), float(c0), _dp(u), _dp(out))
+    finally:
+        lib().nwo_set_true_pmc(0)
     return out
 
 
-def step(m: MeshArrays, c0: float, dt: float, nsteps: int, u: np.ndarray, k=None):
+def step(m: MeshArrays, c0: float, dt: float, nsteps: int, u: np.ndarray, k=None,
+         true_pmc: bool = False):
     """nsteps LSRK45 steps; returns (u, k) as new arrays."""
     u = np.array(u, dtype=np.float64, copy=True)
     k = np.zeros_like(u) if k is None else np.array(k, dtype=np.float64, copy=True)
-    lib().nwo_step(*m.geo_args(), float(c0), float(dt), int(nsteps), _dp(u), _dp(k))
+    lib().nwo_set_true_pmc(int(true_pmc))
+    try:
+        lib().nwo_step(*m.geo_args(), float(c0), float(dt), int(nsteps), _dp(u), _dp(k))
+    finally:
+        lib().nwo_set_true_pmc(0)
     return u, k
 
 

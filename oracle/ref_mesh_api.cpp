@@ -34,6 +34,15 @@ void nwref_mesh_sizes(void* h, long* nelt, long* npts, long* nfp) {
     *nfp = n;
 }
 
+// Node coordinates only (Mesh::getCoordX/Y/Z), for initial states of large meshes.
+void nwref_mesh_coords(void* h, double* x, double* y, double* zc) {
+    const Mesh* m = static_cast<Mesh*>(h);
+    const long npts = m->getTotalPoints();
+    std::memcpy(x, m->getCoordX().data(), sizeof(double) * npts);
+    std::memcpy(y, m->getCoordY().data(), sizeof(double) * npts);
+    std::memcpy(zc, m->getCoordZ().data(), sizeof(double) * npts);
+}
+
 double nwref_mesh_dxmin(void* h) { return static_cast<Mesh*>(h)->computeMinNodeDistance(); }
 
 // Copies the mesh arrays out, face data flattened exactly as

@@ -19,13 +19,14 @@ def record(name: str, data: dict) -> None:
         json.dump(data, f, indent=1)
 
 
-def solver_for(m: "O.MeshArrays", c0: float, precision: str = "fp64") -> DgSolver:
+def solver_for(m: "O.MeshArrays", c0: float, precision: str = "fp64",
+               true_pmc: bool = False) -> DgSolver:
     """libnwb solver on exactly the oracle's mesh arrays."""
     mesh = Mesh.from_arrays(m.N, m.nelt, z=m.z, w=m.w, D=m.D, w3=m.w3, jac=m.jac, met=m.met,
                             vmin=m.vmin, vplus=m.vplus, bc=m.bc, nx=m.nx, ny=m.ny, nz=m.nz,
                             dA=m.dA, x=m.x, y=m.y, zc=m.zc)
     s = DgSolver(precision)
-    s.initialize(mesh, c0)
+    s.initialize(mesh, c0, true_pmc=true_pmc)
     s._keep_mesh = mesh
     return s
 

@@ -403,3 +403,72 @@ def test_nonfinite_state_is_reported_not_hidden(gpu):
     with pytest.raises(NwbError, match="NWB_EINVAL"):
         s.uploadState(u[:-6])
     s.finalize()
+
+
+def _pmc_meshes(N):
+    """Unit cube with PMC (bc 2) walls at x = 0, 1: the axis-aligned class (box
+    elements) and the per-node class (the same walls on a warped mesh)."""
+    from tests.test_pmc_oracle import pmc_x_cube
+    box = pmc_x_cube(N, (3, 2, 2))
+    warped = O.warped_box_mesh(N, (3, 2, 2), warp=0.05)
+    fp = np.arange(warped.nfp)
+    face = (fp // (N * N)) % 6
+    xw = np.isclose(warped.x[warped.vmin], 0.0) | np.isclose(warped.x[warped.vmin], 1.0)
+    warped.bc = warped.bc.copy()
+    warped.bc[((face == 1) | (face == 3)) & xw & (warped.vplus < 0)] = 2
+    return box, warped
+
+
+@pytest.mark.parametrize("N", range(2, 11))
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_true_pmc_option_every_launch_shape(gpu, N, prec):
+    """NWB_SOLVER_TRUE_PMC against the oracle's PMC option (pinned to the analytic
+    PMC cavity mode on the CPU), on every launch shape of the box class and on the
+    per-node class; without the flag the same mesh gives the reference's PEC
+    mapping of bc 2."""
+    box, warped = _pmc_meshes(N)
+    tol = RHS_TOL if prec == "fp64" else 1e-4
+    stol = STEP_TOL if prec == "fp64" else 1e-5
+    for m, geo in ((box, 0), (warped, 2)):
+        assert np.count_nonzero(m.bc == 2) > 0
+        u = random_state(m, 11)
+        dt = 0.5 * O.dxmin(m)
+        for true_pmc in (False, True):
+            s = solver_for(m, 1.0, prec, true_pmc=true_pmc)
+            info = s.info()
+            assert info["geometry"] == geo
+            if true_pmc:  # the structured-box neighbour rule knows PEC walls only
+                assert info["structured"] == (0, 0, 0)
+            want = O.rhs(m, 1.0, u, true_pmc=true_pmc)
+            want_steps, _ = O.step(m, 1.0, dt, 2, u, true_pmc=true_pmc)
+            for v in range(info["variant_count"]):
+                s.setVariant(v)
+                s.uploadState(u)
+                assert rel_max(s.evalRhs(), want) < tol, (geo, true_pmc, v)
+                s.steps(dt, 2)
+                assert rel_l2(s.downloadState(), want_steps) < stol, (geo, true_pmc, v)
+            s.finalize()
+
+
+@pytest.mark.parametrize("N,nel", [(5, (4, 4, 4)), (8, (6, 5, 4))])
+def test_max_norms_equal_the_host_loop_bit_for_bit(gpu, N, nel):
+    """nwb_max_norms against Case::getMaxE/getMaxH (src/case.cpp:768-794) restated
+    in numpy (elementwise roundings, no contraction): equal bit for bit, also with
+    a NaN node, which the host's comparison passes over."""
+    m = O.box_mesh(N, nel, (0, 0, 0), (1, 1, 1))
+    s = solver_for(m, 1.0)
+    u = random_state(m, 21)
+    n = m.npts
+
+    def host(u):
+        c = u.reshape(6, n)
+        e = np.sqrt((c[0] * c[0] + c[1] * c[1]) + c[2] * c[2])
+        h = np.sqrt((c[3] * c[3] + c[4] * c[4]) + c[5] * c[5])
+        return float(np.nanmax(e)), float(np.nanmax(h))
+
+    s.uploadState(u)
+    assert s.maxNorms() == host(u)
+    u[4 * n + 17] = np.nan
+    s.uploadState(u)
+    assert s.maxNorms() == host(u)
+    s.finalize()
