@@ -103,6 +103,15 @@ nwb_status nwb_box_mesh_gll(const nwb_box_mesh* m, const double** z, const doubl
 /* Smallest GLL node spacing, Mesh::computeMinNodeDistance (src/mesh.cpp:883-930). */
 nwb_status nwb_box_mesh_dxmin(const nwb_box_mesh* m, double* dxmin);
 void nwb_box_mesh_destroy(nwb_box_mesh* m);
+/* ProbeManager::init (src/probe.cpp:33-96) on the box mesh of these parameters,
+ * on the host: for probe q at xyz[3q..3q+2], elem[q] = the first element whose box
+ * is nearest (reference coordinates clamped to [-1,1]) and weights[(3q+a)*N + i]
+ * the 1-D Lagrange weights along axis a (r, s, t); the tensor weight of node
+ * (i,j,k) is w_r[i] w_s[j] w_t[k], the reference's interpWeights.  This is how
+ * nwb_pool_add_box places its probes. */
+nwb_status nwb_box_probes(int N, int nelx, int nely, int nelz, double xmin, double xmax,
+                          double ymin, double ymax, double zmin, double zmax, int nprobes,
+                          const double* xyz, int* elem, double* weights);
 
 /* ---- single-mesh solver: DgSolver (src/dg_solver.hpp:35-102) -----------------
  * nwb_solver_create     <- DgSolver::initialize(mesh, c0)   (src/dg_solver.cpp:40)
@@ -139,6 +148,14 @@ nwb_status nwb_solver_init_pulse(nwb_solver* s, const double* pulse /* [30] */);
 /* n must be 6*npts (the reference asserts the same, src/dg_solver.cpp:244). */
 nwb_status nwb_upload_state(nwb_solver* s, const double* host_state, size_t n);
 nwb_status nwb_download_state(nwb_solver* s, double* host_state, size_t n);
+/* Part of DgSolver::downloadState (src/dg_solver.cpp:264-283): nodes
+ * [first, first+count) of all six components into their places of the
+ * 6*npts-double host state (n = 6*npts); the rest of host_state is left as it
+ * is.  For a front end that needs only some elements every step (the probe
+ * elements of ProbeManager::record, src/probe.cpp:192-216) instead of the full
+ * per-step download of Case::simulate (src/case.cpp:588).  Synchronous. */
+nwb_status nwb_download_nodes(nwb_solver* s, long long first, long long count, double* host_state,
+                              size_t n);
 /* Enqueues nsteps LSRK45 steps of size dt on the solver's stream and returns
  * without waiting (the reference's step blocks; nwb_sync restores that). */
 nwb_status nwb_step(nwb_solver* s, double dt, int nsteps);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "nwb_box_mesh_gll": (C.c_int, [C.c_void_p] + [C.POINTER(_D)] * 2),
     "nwb_box_mesh_dxmin": (C.c_int, [C.c_void_p, _D]),
     "nwb_box_mesh_destroy": (None, [C.c_void_p]),
+    "nwb_box_probes": (C.c_int, [C.c_int] * 4 + [C.c_double] * 6 + [C.c_int, _D, _I, _D]),
     "nwb_solver_create": (C.c_int, [C.POINTER(MeshDesc), C.c_double, C.c_int,
                                     C.POINTER(C.c_void_p)]),
     "nwb_solver_create_ex": (C.c_int, [C.POINTER(MeshDesc), C.c_double, C.c_int, C.c_uint,
@@ -76,6 +77,7 @@ SIGNATURES = {
     "nwb_solver_init_pulse": (C.c_int, [C.c_void_p, _D]),
     "nwb_upload_state": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_download_state": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
+    "nwb_download_nodes": (C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, _D, C.c_size_t]),
     "nwb_step": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "nwb_sync": (C.c_int, [C.c_void_p]),
     "nwb_eval_rhs": (C.c_int, [C.c_void_p, _D, C.c_size_t]),

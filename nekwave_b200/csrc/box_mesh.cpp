@@ -529,4 +529,31 @@ nwb_status nwb_box_mesh_dxmin(const nwb_box_mesh* m, double* out) {
 
 void nwb_box_mesh_destroy(nwb_box_mesh* m) { delete m; }
 
+// ProbeManager::init (src/probe.cpp:33-96) on a box mesh: the probes'
+// elements and 1-D Lagrange weights, as the pool locates them.
+nwb_status nwb_box_probes(int N, int nelx, int nely, int nelz, double xmin, double xmax, double ymin,
+                          double ymax, double zmin, double zmax, int nprobes, const double* xyz,
+                          int* elem, double* weights) {
+    if (N < 2 || N > 10 || nelx < 1 || nely < 1 || nelz < 1 || nprobes < 0 ||
+        (nprobes > 0 && (!xyz || !elem || !weights)) || !(xmax > xmin) || !(ymax > ymin) ||
+        !(zmax > zmin)) {
+        nwb_set_error_("nwb_box_probes: bad argument");
+        return NWB_EINVAL;
+    }
+    try {
+        std::vector<double> z, w, D;
+        nwb::gll(N, z, w, D);
+        const double lo[3] = {xmin, ymin, zmin}, hi[3] = {xmax, ymax, zmax};
+        std::vector<int> el;
+        std::vector<double> wt;
+        nwb::box_probes(N, nelx, nely, nelz, lo, hi, z, nprobes, xyz, el, wt);
+        std::copy(el.begin(), el.end(), elem);
+        std::copy(wt.begin(), wt.end(), weights);
+    } catch (const std::bad_alloc&) {
+        nwb_set_error_("nwb_box_probes: out of host memory");
+        return NWB_ENOMEM;
+    }
+    return NWB_OK;
+}
+
 }  // extern "C"

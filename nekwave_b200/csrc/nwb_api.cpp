@@ -696,6 +696,21 @@ nwb_status nwb_download_state(nwb_solver* s, double* h, size_t n) {
     return NWB_OK;
 }
 
+nwb_status nwb_download_nodes(nwb_solver* s, long long first, long long count, double* h, size_t n) {
+    if (!s || !h) return fail(NWB_EINVAL, "nwb_download_nodes: null argument");
+    if (n != 6 * static_cast<size_t>(s->npts))
+        return fail(NWB_EINVAL, "nwb_download_nodes: size %zu, expected 6*npts = %lld", n, 6 * s->npts);
+    if (first < 0 || count < 0 || first + count > s->npts)
+        return fail(NWB_EINVAL, "nwb_download_nodes: nodes [%lld, %lld) outside [0, %lld)", first,
+                    first + count, s->npts);
+    if (count == 0) return NWB_OK;
+    NWB_CU(cudaMemcpy2DAsync(h + first, sizeof(double) * s->npts, s->u[s->cur] + first,
+                             sizeof(double) * s->stride, sizeof(double) * count, 6,
+                             cudaMemcpyDeviceToHost, s->st));
+    NWB_CU(cudaStreamSynchronize(s->st));
+    return NWB_OK;
+}
+
 nwb_status nwb_step(nwb_solver* s, double dt, int nsteps) {
     if (!s) return fail(NWB_EINVAL, "nwb_step: null solver");
     if (nsteps < 0 || !std::isfinite(dt)) return fail(NWB_EINVAL, "nwb_step: bad dt/nsteps");

@@ -12,6 +12,9 @@
 //   DgSolver::step          -> nwb_step + nwb_sync   (src/dg_solver.cpp:306-527)
 //   DgSolver::finalize      -> nwb_solver_destroy    (src/dg_solver.cpp:529-582)
 //
+// It also implements device_diag.hpp, the device diagnostics a front end calls
+// in place of its per-step full download and host reductions.
+//
 // The face points are handed over in the canonical (element, face, q, p) order
 // nwb_mesh_desc requires; Mesh::getFaceData lists them per (element, face) in
 // the order of Mesh::m_faces, so they are re-ordered by (elementId, faceId).
@@ -20,14 +23,18 @@
 // the reference): NWB_PRECISION=fp32 selects the FP32-bulk class,
 // NWB_AUTOTUNE=1 times the stage kernel's launch shapes at initialize.
 #include "dg_solver.hpp"
+#include "device_diag.hpp"
 #include "mesh.hpp"
 #include "nwb.h"
+#include "probe.hpp"
 
 #include <cuda_runtime.h>
 
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -147,6 +154,8 @@ public:
         }
     }
 
+    nwb_solver* handle() const { return s_; }
+
 private:
     nwb_solver* need() const {
         if (!s_) {
@@ -159,10 +168,56 @@ private:
     size_t npts_ = 0;
 };
 
+// libnwb handle of each live DgSolver, for the device diagnostics below (the
+// reference's header gives free functions no access to the pimpl).
+namespace {
+std::mutex g_reg_mu;
+std::map<const DgSolver*, nwb_solver*> g_reg;
+void reg_set(const DgSolver* d, nwb_solver* s) {
+    std::lock_guard<std::mutex> lock(g_reg_mu);
+    if (s) g_reg[d] = s;
+    else g_reg.erase(d);
+}
+nwb_solver* reg_get(const DgSolver& d, const char* what) {
+    std::lock_guard<std::mutex> lock(g_reg_mu);
+    auto it = g_reg.find(&d);
+    if (it == g_reg.end()) {
+        std::fprintf(stderr, "[NekWave nwb ERROR] %s: DgSolver not initialized\n", what);
+        std::abort();
+    }
+    return it->second;
+}
+}  // namespace
+
 DgSolver::DgSolver() : impl_(new Impl()) {}
-DgSolver::~DgSolver() = default;
-bool DgSolver::initialize(const Mesh& mesh, double c0) { return impl_->initialize(mesh, c0); }
+DgSolver::~DgSolver() { reg_set(this, nullptr); }
+bool DgSolver::initialize(const Mesh& mesh, double c0) {
+    const bool ok = impl_->initialize(mesh, c0);
+    reg_set(this, impl_->handle());
+    return ok;
+}
 void DgSolver::uploadState(const double* s, size_t n) { impl_->uploadState(s, n); }
 void DgSolver::downloadState(double* s, size_t n) const { impl_->downloadState(s, n); }
 void DgSolver::step(double dt, double t) { impl_->step(dt, t); }
-void DgSolver::finalize() { impl_->freeBuffers(); }
+void DgSolver::finalize() {
+    reg_set(this, nullptr);
+    impl_->freeBuffers();
+}
+
+namespace nwb_dropin {
+
+void download_probe_elements(const DgSolver& solver, const ProbeManager& probes, int nodes_per_elem,
+                             std::vector<double>& state) {
+    nwb_solver* s = reg_get(solver, "download_probe_elements");
+    for (const ProbePoint& p : probes.getProbes())
+        nwb_or_abort(nwb_download_nodes(s, p.elemOffset, nodes_per_elem, state.data(), state.size()),
+                     "download_probe_elements");
+}
+
+void device_diagnostics(const DgSolver& solver, double* max_e, double* max_h, double* energy) {
+    nwb_solver* s = reg_get(solver, "device_diagnostics");
+    nwb_or_abort(nwb_max_norms(s, max_e, max_h), "device_diagnostics (max norms)");
+    nwb_or_abort(nwb_energy(s, energy), "device_diagnostics (energy)");
+}
+
+}  // namespace nwb_dropin

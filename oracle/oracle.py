@@ -89,8 +89,26 @@ def ref():
                                  _D, _D, _D, _D, C.c_double, C.c_double, C.c_int, _D, _D,
                                  C.c_int]
         L.nwref_threads.restype = C.c_int
+        L.nwref_probe_init.argtypes = [C.c_void_p, C.c_int, _D, C.POINTER(C.c_long), _D]
         _ref = L
     return _ref
+
+
+def ref_probes(N, nel, lo, hi, points):
+    """The reference's own ProbeManager::init (src/probe.cpp:33-96) on its own box
+    Mesh: (element offsets [P], tensor weights [P, N^3])."""
+    L = ref()
+    h = L.nwref_mesh_box(N, nel[0], nel[1], nel[2], lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 0, 0, 0)
+    if not h:
+        raise ValueError("reference createBoxMesh failed")
+    try:
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        off = np.zeros(len(pts), dtype=np.int64)
+        w = np.zeros((len(pts), N ** 3))
+        L.nwref_probe_init(h, len(pts), _dp(pts), off.ctypes.data_as(C.POINTER(C.c_long)), _dp(w))
+    finally:
+        L.nwref_mesh_free(h)
+    return off, w
 
 
 def ref_gpu_available() -> bool:

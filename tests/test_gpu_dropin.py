@@ -88,3 +88,64 @@ def test_reference_cli_end_to_end_against_dropin(gpu, tmp_path):
     record("cli_e2e.json", {"case": "periodic 32^3, 8 points, central, 50 steps, Case::simulate",
                             "reference_wall_s": out["reference"]["wall_s"],
                             "dropin_wall_s": out["dropin"]["wall_s"]})
+
+
+PULSE_REF = os.path.join(ROOT, "oracle", "_ref", "pulse-case-ref")
+
+
+@pytest.mark.skipif(not (os.path.exists(PULSE_REF) and
+                         os.path.exists(os.path.join(DROPIN, "pulse-case-devdiag"))),
+                    reason="pulse-case drivers not built")
+def test_device_diagnostics_front_end_on_a_nonzero_wave(gpu, tmp_path):
+    """The reference's Case::simulate on a seeded Gaussian pulse (the benchmark
+    workload: periodic 32^3, 8 points, central, CFL 0.5), 100 steps, 4 probes,
+    diagnostics every 10 steps, run three ways: the reference's own CUDA build,
+    the drop-in on libnwb with the reference's per-step full download and host
+    diagnostics, and the drop-in with the device-diagnostics Case (probe elements
+    only per step, max|E|, max|H| and energy reduced on the device, full state at
+    save steps and at the end).  The energy histories (step, time, max|E|, max|H|,
+    energy) and probe histories agree to the 9 significant digits the front end
+    prints; the simulate() wall times are recorded (cli_devdiag.json)."""
+    from nekwave_b200.workloads import single_mesh
+    spec = single_mesh("c2", 32, 0)
+    comp, (amp, x0, y0, z0, sig) = 2, spec["pulses"][2]
+    case = {"mesh": {"nelx": 32, "nely": 32, "nelz": 32, "xmin": 0.0, "xmax": 1.0, "ymin": 0.0,
+                     "ymax": 1.0, "zmin": 0.0, "zmax": 1.0, "periodic": "all"},
+            "numerics": {"order": 8, "cfl": 0.5, "flux_type": "central"},
+            "time": {"num_steps": 100},
+            "probes": [[0.31, 0.52, 0.47], [0.5, 0.5, 0.5], [0.77, 0.13, 0.9], [0.05, 0.95, 0.6]],
+            "output": {"output_frequency": 10, "export_fields": False, "export_format": "csv"}}
+    runs = {"reference": PULSE_REF, "dropin": os.path.join(DROPIN, "pulse-case"),
+            "devdiag": os.path.join(DROPIN, "pulse-case-devdiag")}
+    out = {}
+    for name, exe in runs.items():
+        d = tmp_path / name
+        d.mkdir()
+        c = dict(case)
+        c["output"] = dict(case["output"], output_dir=str(d / "out"))
+        p = d / "case.json"
+        p.write_text(json.dumps(c))
+        r = subprocess.run([exe, str(p), str(comp), repr(x0), repr(y0), repr(z0), repr(sig)],
+                           capture_output=True, text=True, timeout=900, cwd=d)
+        assert r.returncode == 0, name + ": " + r.stdout[-2000:] + r.stderr[-2000:]
+        sim = [ln for ln in r.stdout.splitlines() if ln.startswith("[pulse-case] simulate_s")]
+        hist = [[float(v) for v in row] for row in list(csv.reader(open(d / "out" / "energy_history.csv")))[1:]]
+        probes = [[float(v) for v in row] for row in list(csv.reader(open(d / "out" / "probe_history.csv")))[1:]]
+        out[name] = dict(simulate_s=float(sim[0].split()[-1]), hist=hist, probes=probes)
+    ref = out["reference"]
+    assert len(ref["hist"]) == 11 and len(ref["probes"]) == 101
+    assert ref["hist"][-1][2] > 0.1 and ref["hist"][-1][4] > 0  # a nonzero wave throughout
+    for name in ("dropin", "devdiag"):
+        for key in ("hist", "probes"):
+            a, b = ref[key], out[name][key]
+            assert len(a) == len(b), (name, key)
+            scale = max(abs(v) for row in a for v in row[2:])
+            for ra, rb in zip(a, b):
+                assert ra[:2] == rb[:2], (name, key, ra[:2], rb[:2])
+                for va, vb in zip(ra[2:], rb[2:]):
+                    # printed to 9 digits; FP64 paths agree to ~1e-14 of the largest value
+                    assert abs(va - vb) <= 2e-8 * abs(va) + 1e-12 * scale, (name, key, va, vb)
+    record("cli_devdiag.json", {
+        "case": "periodic 32^3, 8 points, central, seeded Gaussian Ez, 100 steps, 4 probes, "
+                "diagnostics every 10 steps, Case::simulate",
+        **{f"{k}_simulate_s": v["simulate_s"] for k, v in out.items()}})
