@@ -264,11 +264,16 @@ nwb_status nwb_time_stage_kernel(nwb_solver* s, double dt, int nstages, float* m
  * (Case::simulate, src/case.cpp:529-660).  A pool owns a fixed HBM arena of
  * hbm_budget_bytes, allocated once at creation; every cavity ("slot") is
  * sub-allocated from it, so nwb_pool_add never calls cudaMalloc and returns
- * NWB_EBUSY when the cavity does not fit (admission by HBM budget).
+ * NWB_EBUSY when the cavity does not fit (admission by HBM budget).  Outside the
+ * arena the pool holds its slot table and two work lists (sized at creation for
+ * any admissible set of cavities: 16 bytes each per 18 KB of budget at most) and
+ * a pinned host staging area (2 x 48 MB).  nwb_pool_add, _add_box, _init_pulse,
+ * _upload (states up to 48 MB), _remove and _step queue their device work in
+ * stream order and return without waiting for the steps already in flight.
  * nwb_pool_step advances every uploaded, unfinished slot by up to nsteps steps
- * with one persistent launch per LSRK stage (whatever each slot's N and element
- * count), replayed from one CUDA graph per step; a slot stops by itself after
- * its own nsteps.  Slots take axis-aligned box meshes (nwb_mesh_desc as above),
+ * with one launch per LSRK stage and N present (or one persistent launch for
+ * every N, nwb_pool_set_mode), replayed from one CUDA graph per step; a slot stops
+ * by itself after its own nsteps.  Slots take axis-aligned box meshes (nwb_mesh_desc as above),
  * their own c0 and dt, up to 8 probes given as (element, tensor Lagrange
  * weights [3][N]) as ProbeManager builds them (src/probe.cpp:33-189), and record
  * the energy every energy_every steps (index 0 = initial state, NaN where not
@@ -301,6 +306,21 @@ nwb_status nwb_pool_sync(nwb_pool* p);
 nwb_status nwb_pool_query(nwb_pool* p, int* status, int* done, int cap);
 /* Any of state [6*npts], energy [nsteps+1], probes [(nsteps+1)*nprobes*6] may be NULL. */
 nwb_status nwb_pool_results(nwb_pool* p, int slot, double* state, double* energy, double* probes);
+/* The same status without waiting for the steps in flight: nwb_pool_query_begin
+ * queues a copy of the device slot table after everything queued so far and
+ * returns; nwb_pool_query_end waits for that copy only (later steps keep
+ * running) and reports the status as of that point, as nwb_pool_query does.
+ * Slots admitted after the begin are reported as not yet started (0) or running
+ * (1).  One snapshot is in flight at a time.  No counterpart in the reference. */
+nwb_status nwb_pool_query_begin(nwb_pool* p);
+nwb_status nwb_pool_query_end(nwb_pool* p, int* status, int* done, int cap);
+/* nwb_pool_results without waiting: queues the copies of a slot that the last
+ * nwb_pool_query_end reported finished and returns.  The buffers (pinned host
+ * memory for the copies to be asynchronous) are complete when a later
+ * nwb_pool_query_end or nwb_pool_sync returns; the slot may be removed at once
+ * (its memory is reused only by work queued after the copies). */
+nwb_status nwb_pool_results_async(nwb_pool* p, int slot, double* state, double* energy,
+                                  double* probes);
 nwb_status nwb_pool_remove(nwb_pool* p, int slot);
 nwb_status nwb_pool_info(const nwb_pool* p, size_t* used_bytes, size_t* budget_bytes,
                          int* slots_used, long long* launches);

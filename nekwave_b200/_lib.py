@@ -108,6 +108,9 @@ SIGNATURES = {
     "nwb_pool_sync": (C.c_int, [C.c_void_p]),
     "nwb_pool_query": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
     "nwb_pool_results": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
+    "nwb_pool_query_begin": (C.c_int, [C.c_void_p]),
+    "nwb_pool_query_end": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
+    "nwb_pool_results_async": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
     "nwb_pool_remove": (C.c_int, [C.c_void_p, C.c_int]),
     "nwb_pool_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                 _I, C.POINTER(C.c_longlong)]),

@@ -11,6 +11,7 @@
 #include "stage_kernel.cuh"
 #include "stage_pipe.cuh"
 #include "stage_dmma.cuh"
+#include "stage_bulk.cuh"
 
 namespace nwb {
 namespace {
@@ -132,6 +133,7 @@ batch_stage_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict
         P.flift = nullptr;
         P.fplus = nullptr;
         P.nfp = 0;
+        P.err = nullptr;
         P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
         P.spmask = 0;
         for (int x = 0; x < 10; ++x) P.zl[x] = S.zl[x];
@@ -172,6 +174,7 @@ __device__ __forceinline__ StageParams slot_params(const SlotDev& S, int stage, 
     P.flift = nullptr;
     P.fplus = nullptr;
     P.nfp = 0;
+    P.err = nullptr;
     P.snel[0] = P.snel[1] = P.snel[2] = 0;  // connections from the slot's table
     P.spmask = 0;
     for (int x = 0; x < 10; ++x) P.zl[x] = S.zl[x];
@@ -250,6 +253,41 @@ template <> struct NShape<8> { static constexpr int KS = 2, EPB = 1, KSM = 0, MI
 template <> struct NShape<9> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 12; };
 template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, MINB = 2, ALG = 0; };
 
+// FP64 per-N shapes that run the bulk-copy one-tile form (the single-mesh default
+// at these N): k staged in shared memory, CD = t-derivative D from the parameters.
+// EARLY = neighbour traces requested while the tile's copies fly.
+template <int N> struct NBulk { static constexpr bool on = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1; };
+template <> struct NBulk<5> { static constexpr bool on = true, CD = false, EARLY = false; static constexpr int EPB = 2, MINB = 4; };
+template <> struct NBulk<6> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3; };
+template <> struct NBulk<7> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4; };
+template <> struct NBulk<9> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2; };
+
+template <int N, bool CD>
+__global__ void __launch_bounds__(NBulk<N>::EPB * 2 * N * N, NBulk<N>::MINB)
+batch_bulk_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restrict__ work, int stage,
+                    int dry, const __grid_constant__ DParam dp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WorkItem w = work[blockIdx.x];
+    const SlotDev& S = slots[w.slot];
+    if (!S.active) return;
+    const StageParams P = slot_params(S, stage, dry);
+    stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY>(P, w.e0, smem,
+                                                                                      threadIdx.x, dp.d);
+}
+
+template <int N, bool CD>
+cudaError_t launch_bulk_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
+                          const DParam& dp, cudaStream_t st) {
+    constexpr int smem = stage::BulkLayout<N, NBulk<N>::EPB, true>::total;
+    constexpr int threads = NBulk<N>::EPB * 2 * N * N;
+    auto kern = batch_bulk_n_kernel<N, CD>;
+    static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
+    if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;
+    if (ntiles <= 0) return cudaSuccess;
+    kern<<<ntiles, threads, smem, st>>>(slots, work, stage, dry, dp);
+    return cudaGetLastError();
+}
+
 template <int N, bool F32, int ALG>
 cudaError_t launch_n_alg(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
                          const DParam& dp, cudaStream_t st) {
@@ -273,6 +311,21 @@ cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int 
                      const double* Dh, cudaStream_t st, int* epb_out) {
     using Sh = NShape<N>;
     if (epb_out) *epb_out = Sh::EPB;
+    if constexpr (NBulk<N>::on && !F32) {
+        static_assert(NBulk<N>::EPB == Sh::EPB, "the per-N work list is cut with NShape's EPB");
+        DParam dp{};
+        if constexpr (NBulk<N>::CD) {
+            if (Dh) {
+                for (int x = 0; x < N * N; ++x) dp.d[x] = Dh[x];
+                return launch_bulk_n<N, true>(stage, slots, work, ntiles, dry, dp, st);
+            }
+            if (ntiles <= 0) {  // set-up call: prepare both forms
+                cudaError_t e = launch_bulk_n<N, true>(stage, slots, work, 0, dry, dp, st);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        return launch_bulk_n<N, false>(stage, slots, work, ntiles, dry, dp, st);
+    }
     if constexpr (dmma_tile<N, F32>()) {
         DParam dp{};
         if (Dh) {

@@ -245,6 +245,7 @@ struct nwb_solver {
     double* dw3 = nullptr;
     double* dpartial = nullptr;
     double* denergy = nullptr;
+    int* derr = nullptr;  // kernels record an expired bounded wait here
     int eblocks = 1;
     void* dflush = nullptr;
     size_t flush_bytes = 0;
@@ -272,6 +273,7 @@ struct nwb_solver {
         P.flift = dflift;
         P.fplus = dfplus;
         P.nfp = nfp;
+        P.err = derr;
         P.c0 = c0;
         P.a = kRK4A[stage];
         P.b = kRK4B[stage];
@@ -363,7 +365,8 @@ struct nwb_solver {
     void release() {
         drop_graphs();
         void* ptrs[] = {u[0], u[1], k, dD, dgeo, dconn, djac_e, dmet_n, dfnrm, dflift,
-                        dfplus, djac_n, dw3, dpartial, denergy, dflush, dprobe_off, dprobe_w, dprobe_out, dsnap};
+                        dfplus, djac_n, dw3, dpartial, denergy, dflush, dprobe_off, dprobe_w, dprobe_out, dsnap,
+                        derr};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -555,6 +558,9 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
     // partial sums of the energy, or (max|E|, max|H|) pairs; energy, max|E|, max|H|
     NWB_TRY(dalloc(&s->dpartial, 2 * static_cast<size_t>(s->eblocks), &tot));
     NWB_TRY(dalloc(&s->denergy, 3, &tot));
+    NWB_TRY(dalloc(&s->derr, 1, &tot));
+    ce = cudaMemset(s->derr, 0, sizeof(int));
+    if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "memset: %s", cudaGetErrorString(ce)));
 #define NWB_H2D(dst, src, bytes) \
     do { ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
          if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "upload: %s", cudaGetErrorString(ce))); } while (0)
@@ -564,10 +570,14 @@ nwb_status create_solver(const nwb_mesh_desc* m, int N, int nelt, const double* 
     NWB_H2D(s->dw3, w3, sizeof(double) * N3);
     if (s->geo != nwb::GEO_NODAL) {
         NWB_TRY(dalloc(&s->dgeo, static_cast<size_t>(nelt), &tot));
-        NWB_TRY(dalloc(&s->dconn, 6 * static_cast<size_t>(nelt), &tot));
+        // padded to a multiple of four entries: bulk copies of a tile's connections
+        // are 16-byte aligned at both ends (stage_ws.cuh)
+        NWB_TRY(dalloc(&s->dconn, 6 * static_cast<size_t>(nelt) + 4, &tot));
         NWB_TRY(dalloc(&s->djac_e, static_cast<size_t>(nelt), &tot));
         NWB_H2D(s->dgeo, A.egeo.data(), sizeof(nwb::ElemGeo) * nelt);
         NWB_H2D(s->dconn, A.conn.data(), sizeof(int) * 6 * static_cast<size_t>(nelt));
+        ce = cudaMemset(s->dconn + 6 * static_cast<size_t>(nelt), 0, 4 * sizeof(int));
+        if (ce != cudaSuccess) return bail(fail(NWB_ECUDA, "memset: %s", cudaGetErrorString(ce)));
         NWB_H2D(s->djac_e, A.jac_e.data(), sizeof(double) * nelt);
         detect_structure(A.conn, nelt, s->snel, &s->spmask);
     } else {
@@ -721,6 +731,14 @@ nwb_status nwb_step(nwb_solver* s, double dt, int nsteps) {
 nwb_status nwb_sync(nwb_solver* s) {
     if (!s) return fail(NWB_EINVAL, "nwb_sync: null solver");
     NWB_CU(cudaStreamSynchronize(s->st));
+    // a bounded wait inside a stage kernel that expired (the warp-specialised form)
+    int err = 0;
+    NWB_CU(cudaMemcpy(&err, s->derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err != 0) {
+        NWB_CU(cudaMemset(s->derr, 0, sizeof(int)));
+        return fail(NWB_ETIMEOUT, "nwb_sync: a stage kernel's bounded wait expired (code %d); the "
+                                  "state of the steps since the last sync is not valid", err);
+    }
     return NWB_OK;
 }
 
@@ -894,7 +912,8 @@ nwb_status nwb_solver_set_variant(nwb_solver* s, int variant) {
         return fail(NWB_EINVAL, "nwb_solver_set_variant: variant %d out of range", variant);
     nwb::StageConfig c{};
     cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, variant, nullptr, nullptr, &c);
-    if (e != cudaSuccess) return fail(NWB_ECUDA, "variant set-up: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        return fail(NWB_ECUDA, "variant %d set-up: %s", variant, cudaGetErrorString(e));
     NWB_CU(cudaStreamSynchronize(s->st));
     s->variant = variant;
     s->cfg = c;
@@ -917,7 +936,7 @@ nwb_status nwb_solver_autotune(nwb_solver* s, int reps, int* best, float* ms_out
     for (int v = 0; v < nv; ++v) {
         nwb::StageConfig c{};
         cudaError_t e = nwb::launch_stage(s->N, s->geo, s->f32, v, nullptr, nullptr, &c);
-        if (e != cudaSuccess) return fail(NWB_ECUDA, "variant set-up: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) return fail(NWB_ECUDA, "variant %d set-up: %s", v, cudaGetErrorString(e));
         nwb::StageParams P = s->params(0, 0.0);
         P.a = 0.0;
         P.b = 0.0;

@@ -79,6 +79,8 @@ struct StageParams {
     const double* flift;    // [nfp]        (GEO_NODAL)
     const int* fplus;       // [nfp] neighbour node, -1 mirror (GEO_NODAL)
     long long nfp;
+    int* err;               // device status word: a kernel whose bounded wait expires
+                            // records a nonzero code here (null: none kept)
     double c0;              // flux penalty: 0 central, 1 upwind
     double a, b, dt;        // LSRK45 stage coefficients and step
     int snel[3];            // structured box mesh: elements per axis (x fastest), or 0

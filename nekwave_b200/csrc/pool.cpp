@@ -5,7 +5,13 @@
 // active ones with one persistent launch per LSRK stage (batch.cu):
 //   * admission by a fixed HBM budget: the pool owns one arena allocated at
 //     creation and sub-allocates every slot's buffers from it, so admitting a
-//     cavity never calls cudaMalloc and fails with NWB_EBUSY when it does not fit;
+//     cavity never calls cudaMalloc and fails with NWB_EBUSY when it does not fit
+//     (the slot table and the work lists, sized at creation for any admissible
+//     set of cavities, live outside the arena);
+//   * no host waits on the admission path: host data goes through pinned
+//     staging and every copy is queued in stream order behind the steps in
+//     flight; status and results can be read back the same way
+//     (nwb_pool_query_begin/end, nwb_pool_results_async);
 //   * a step of all slots is one CUDA graph (5 stage launches, diagnostics,
 //     step epilogue) replayed as often as needed; slots that have taken their
 //     steps fall idle on the device, and slots can be added or removed between
@@ -90,8 +96,66 @@ private:
     size_t total_ = 0, used_ = 0;
 };
 
+// Pinned host staging for the pool's host-to-device copies.  A copy from pageable
+// memory makes the CUDA runtime wait for everything already queued on the stream
+// (the steps of the resident cavities), so admissions, uploads of slot records
+// and work lists first copy their data here and then queue a truly asynchronous
+// copy.  Two chunks are used in turn; before a chunk is reused, the copies queued
+// from it are waited for (an event recorded after them), which in steady state
+// have long finished.
+class Staging {
+public:
+    static constexpr size_t kChunk = 48u << 20;  // a 48^3-element box cavity's geometry fits
+    cudaError_t init() {
+        for (int c = 0; c < 2; ++c) {
+            cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&buf_[c]), kChunk, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_[c], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    void destroy() {
+        for (int c = 0; c < 2; ++c) {
+            if (buf_[c]) cudaFreeHost(buf_[c]);
+            if (ev_[c]) cudaEventDestroy(ev_[c]);
+            buf_[c] = nullptr;
+            ev_[c] = nullptr;
+        }
+    }
+    // Pinned space for bytes; nullptr when they exceed a chunk (the caller then
+    // copies from its own memory and synchronises).  Copies from the space must be
+    // queued on st before the next call.
+    void* get(size_t bytes, cudaStream_t st) {
+        bytes = (bytes + 15) & ~static_cast<size_t>(15);
+        if (bytes > kChunk) return nullptr;
+        if (used_ + bytes > kChunk) {
+            if (cudaEventRecord(ev_[cur_], st) != cudaSuccess) return nullptr;
+            live_[cur_] = true;
+            cur_ ^= 1;
+            if (live_[cur_] && cudaEventSynchronize(ev_[cur_]) != cudaSuccess) return nullptr;
+            used_ = 0;
+        }
+        void* p = buf_[cur_] + used_;
+        used_ += bytes;
+        return p;
+    }
+    // Marks the copies queued so far from the current chunk.
+    cudaError_t mark(cudaStream_t st) {
+        live_[cur_] = true;
+        return cudaEventRecord(ev_[cur_], st);
+    }
+
+private:
+    char* buf_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
+    bool live_[2] = {false, false};
+    int cur_ = 0;
+    size_t used_ = 0;
+};
+
 struct SlotHost {
     bool used = false;
+    unsigned gen = 0;     // admission generation: status snapshots of an older one are ignored
     bool dcanon = false;  // its D equals the pool's D for its N (the GLL operator)
     bool uploaded = false;
     bool is_box = false;
@@ -135,6 +199,14 @@ struct nwb_pool {
     int grid = 0, diag_grid = 0;
     int sms = 148;
     long long launches = 0;
+    Staging stage;
+    // asynchronous status snapshots (nwb_pool_query_begin/end): the device slot
+    // table copied into pinned memory, and each slot's generation when it was taken
+    nwb::SlotDev* h_snap = nullptr;
+    cudaEvent_t snap_ev = nullptr;
+    bool snap_pending = false;
+    std::vector<unsigned> snap_gen;
+    unsigned next_gen = 1;
 
     template <class T>
     T* ptr(const Range& r) const {
@@ -147,14 +219,24 @@ struct nwb_pool {
         graph_smem = -1;
     }
 
-    nwb_status write_slot(int s) {
-        NWB_PCU(cudaMemcpyAsync(d_slots + s, &slots[s].dev, sizeof(nwb::SlotDev),
-                                cudaMemcpyHostToDevice, st));
-        // the host copy is a member of a live vector and may change before the
-        // copy runs: wait for it here (slot changes are rare, between replays)
-        NWB_PCU(cudaStreamSynchronize(st));
+    // Host-to-device copy of bytes through the pinned staging area (asynchronous);
+    // data larger than a staging chunk is copied directly, with a synchronisation.
+    nwb_status h2d(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return NWB_OK;
+        void* pin = stage.get(bytes, st);
+        if (!pin) {
+            NWB_PCU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+            NWB_PCU(cudaStreamSynchronize(st));
+            return NWB_OK;
+        }
+        std::memcpy(pin, src, bytes);
+        NWB_PCU(cudaMemcpyAsync(dst, pin, bytes, cudaMemcpyHostToDevice, st));
+        NWB_PCU(stage.mark(st));
         return NWB_OK;
     }
+
+    // The device copy of slot s's record, queued in stream order (no host wait).
+    nwb_status write_slot(int s) { return h2d(d_slots + s, &slots[s].dev, sizeof(nwb::SlotDev)); }
 
     // Work list: every tile of every used slot, largest tiles first, so the
     // dynamic tile counter hands out the long tiles early.
@@ -185,28 +267,15 @@ struct nwb_pool {
             }
             n_cnt[N] = static_cast<int>(wn.size()) - n_off[N];
         }
-        if (static_cast<int>(wn.size()) > work_n_cap) {
-            if (d_work_n) cudaFree(d_work_n);
-            d_work_n = nullptr;
-            work_n_cap = std::max(static_cast<int>(wn.size()), 2 * work_n_cap);
-            NWB_PCU(cudaMalloc(&d_work_n, sizeof(nwb::WorkItem) * work_n_cap));
-        }
-        if (!wn.empty())
-            NWB_PCU(cudaMemcpyAsync(d_work_n, wn.data(), sizeof(nwb::WorkItem) * wn.size(),
-                                    cudaMemcpyHostToDevice, st));
+        // both lists were sized at creation for every admissible cavity set
+        if (static_cast<int>(wn.size()) > work_n_cap || ntiles > work_cap)
+            return set_error(NWB_EINVAL, "pool work list: %d tiles over its capacity %d", ntiles,
+                             work_cap);
+        nwb_status r = h2d(d_work_n, wn.data(), sizeof(nwb::WorkItem) * wn.size());
+        if (r == NWB_OK) r = h2d(d_work, w.data(), sizeof(nwb::WorkItem) * ntiles);
+        if (r == NWB_OK) r = h2d(d_ntiles, &ntiles, sizeof(int));
+        if (r != NWB_OK) return r;
         if (mode == 1) drop_graph();  // per-N grids follow the tile counts
-        if (ntiles > work_cap) {
-            if (d_work) cudaFree(d_work);
-            d_work = nullptr;
-            work_cap = std::max(ntiles, 2 * work_cap);
-            drop_graph();
-            NWB_PCU(cudaMalloc(&d_work, sizeof(nwb::WorkItem) * work_cap));
-        }
-        if (ntiles)
-            NWB_PCU(cudaMemcpyAsync(d_work, w.data(), sizeof(nwb::WorkItem) * ntiles,
-                                    cudaMemcpyHostToDevice, st));
-        NWB_PCU(cudaMemcpyAsync(d_ntiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, st));
-        NWB_PCU(cudaStreamSynchronize(st));
         work_dirty = false;
         return NWB_OK;
     }
@@ -332,6 +401,28 @@ nwb_status nwb_pool_create(size_t hbm_budget_bytes, int max_slots, nwb_precision
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join_ev[N], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork_ev, cudaEventDisableTiming);
+    // Work lists sized once for any set of cavities the budget admits: each element
+    // takes at least 3 x 6 x N^3 doubles of the arena (u twice, k), each full tile
+    // holds epb elements, and each slot adds at most one partial tile.  With 2-point
+    // cavities in 16-element tiles that is one 16-byte entry per 18 KB of budget.
+    if (e == cudaSuccess) {
+        double min_tile = 1e300;
+        for (int N = 2; N <= 10; ++N) {
+            const int epb = std::min(nwb::batch_shape(N, p->f32).epb, nwb::batch_epb_n(N));
+            min_tile = std::min(min_tile, 144.0 * N * N * N * epb);
+        }
+        const double cap = static_cast<double>(max_slots) + static_cast<double>(hbm_budget_bytes) / min_tile + 1;
+        if (cap > 0x7fffffff) e = cudaErrorInvalidValue;
+        p->work_cap = p->work_n_cap = static_cast<int>(cap);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_work, sizeof(nwb::WorkItem) * p->work_cap);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_work_n, sizeof(nwb::WorkItem) * p->work_n_cap);
+    if (e == cudaSuccess) e = p->stage.init();
+    if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void**>(&p->h_snap), sizeof(nwb::SlotDev) * max_slots,
+                          cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->snap_ev, cudaEventDisableTiming);
+    p->snap_gen.assign(max_slots, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return bail(set_error(NWB_ECUDA, "nwb_pool_create: %s", cudaGetErrorString(e)));
     *out = p;
@@ -424,26 +515,30 @@ nwb_status admit(nwb_pool* p, int N, int nelt, const double* D, const double* w3
     d.done = 0;
     d.par = 0;
     d.active = 0;  // set when the initial state arrives
-    auto cp = [&](int idx, const void* src, size_t bytes) -> cudaError_t {
-        return bytes ? cudaMemcpyAsync(p->base + h.ranges[idx].off, src, bytes, cudaMemcpyHostToDevice, p->st)
-                     : cudaSuccess;
-    };
+    // queued in stream order after the steps already in flight (the ranges may be
+    // a removed cavity's, which those steps may still read); no host wait
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 3 && e == cudaSuccess; ++b)
         e = cudaMemsetAsync(p->base + h.ranges[b].off, 0, sizes[b], p->st);
-    if (e == cudaSuccess) e = cp(3, D, sizes[3]);
-    if (e == cudaSuccess) e = cp(4, w3, sizes[4]);
-    if (e == cudaSuccess) e = cp(5, egeo, sizes[5]);
-    if (e == cudaSuccess) e = cp(6, conn, sizes[6]);
-    if (e == cudaSuccess && nprobes) e = cp(10, probe_elem, sizeof(int) * nprobes);
-    if (e == cudaSuccess && nprobes) e = cp(11, probe_w, sizeof(double) * 3 * N * nprobes);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(p->st);
-    if (e != cudaSuccess) {
-        for (const Range& q : h.ranges) p->arena.release(q);
-        return set_error(NWB_ECUDA, "nwb_pool_add: %s", cudaGetErrorString(e));
+    nwb_status r = e == cudaSuccess ? NWB_OK : set_error(NWB_ECUDA, "nwb_pool_add: %s", cudaGetErrorString(e));
+    auto cp = [&](int idx, const void* src, size_t bytes) {
+        if (r == NWB_OK) r = p->h2d(p->base + h.ranges[idx].off, src, bytes);
+    };
+    cp(3, D, sizes[3]);
+    cp(4, w3, sizes[4]);
+    cp(5, egeo, sizes[5]);
+    cp(6, conn, sizes[6]);
+    if (nprobes) {
+        cp(10, probe_elem, sizeof(int) * nprobes);
+        cp(11, probe_w, sizeof(double) * 3 * N * nprobes);
     }
+    if (r != NWB_OK) {
+        for (const Range& q : h.ranges) p->arena.release(q);
+        return r;
+    }
+    h.gen = p->next_gen++;
     p->slots[s] = h;
-    nwb_status r = p->write_slot(s);
+    r = p->write_slot(s);
     if (r != NWB_OK) {
         p->release_slot(s);
         return r;
@@ -538,8 +633,14 @@ nwb_status nwb_pool_upload(nwb_pool* p, int s, const double* h, size_t n) {
         return set_error(NWB_EINVAL, "nwb_pool_upload: size %zu, expected 6*npts", n);
     nwb_status r = p->rebuild_work();
     if (r != NWB_OK) return r;
-    NWB_PCU(cudaMemcpy2DAsync(sh.dev.u[0], sizeof(double) * sh.stride, h, sizeof(double) * sh.npts,
-                              sizeof(double) * sh.npts, 6, cudaMemcpyHostToDevice, p->st));
+    const size_t bytes = sizeof(double) * 6 * static_cast<size_t>(sh.npts);
+    void* pin = p->stage.get(bytes, p->st);
+    if (pin) std::memcpy(pin, h, bytes);  // queued without waiting for the steps in flight
+    NWB_PCU(cudaMemcpy2DAsync(sh.dev.u[0], sizeof(double) * sh.stride, pin ? pin : h,
+                              sizeof(double) * sh.npts, sizeof(double) * sh.npts, 6,
+                              cudaMemcpyHostToDevice, p->st));
+    if (pin) NWB_PCU(p->stage.mark(p->st));
+    else NWB_PCU(cudaStreamSynchronize(p->st));
     NWB_PCU(cudaMemsetAsync(sh.dev.k, 0, sizeof(double) * 6 * sh.stride, p->st));
     sh.dev.par = 0;
     sh.dev.done = 0;
@@ -621,6 +722,59 @@ nwb_status nwb_pool_query(nwb_pool* p, int* status, int* done, int cap) {
     return NWB_OK;
 }
 
+nwb_status nwb_pool_query_begin(nwb_pool* p) {
+    if (!p) return set_error(NWB_EINVAL, "nwb_pool_query_begin: null pool");
+    if (p->snap_pending) NWB_PCU(cudaEventSynchronize(p->snap_ev));  // one snapshot in flight
+    for (int s = 0; s < p->max_slots; ++s) p->snap_gen[s] = p->slots[s].used ? p->slots[s].gen : 0;
+    NWB_PCU(cudaMemcpyAsync(p->h_snap, p->d_slots, sizeof(nwb::SlotDev) * p->max_slots,
+                            cudaMemcpyDeviceToHost, p->st));
+    NWB_PCU(cudaEventRecord(p->snap_ev, p->st));
+    p->snap_pending = true;
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_query_end(nwb_pool* p, int* status, int* done, int cap) {
+    if (!p || (!status && !done)) return set_error(NWB_EINVAL, "nwb_pool_query_end: bad argument");
+    if (!p->snap_pending) return set_error(NWB_EINVAL, "nwb_pool_query_end: no nwb_pool_query_begin");
+    NWB_PCU(cudaEventSynchronize(p->snap_ev));
+    p->snap_pending = false;
+    for (int s = 0; s < p->max_slots && s < cap; ++s) {
+        SlotHost& h = p->slots[s];
+        const nwb::SlotDev& d = p->h_snap[s];
+        // a slot admitted or removed since the snapshot was taken: not yet in it
+        const bool current = h.used && p->snap_gen[s] == h.gen;
+        int st = -1;
+        if (h.used) st = (!h.uploaded || !current) ? (h.uploaded ? 1 : 0) : (d.done >= d.nsteps ? 2 : 1);
+        if (current) {
+            h.dev.done = d.done;
+            h.dev.par = d.par;
+            h.dev.active = d.active;
+        }
+        if (status) status[s] = st;
+        if (done) done[s] = current ? d.done : 0;
+    }
+    return NWB_OK;
+}
+
+nwb_status nwb_pool_results_async(nwb_pool* p, int s, double* state, double* energy, double* probes) {
+    if (!p || s < 0 || s >= p->max_slots) return set_error(NWB_EINVAL, "nwb_pool_results_async: bad argument");
+    SlotHost& h = p->slots[s];
+    if (!h.used) return set_error(NWB_ENOTFOUND, "nwb_pool_results_async: slot %d is free", s);
+    if (h.dev.done < h.nsteps)
+        return set_error(NWB_EINVAL, "nwb_pool_results_async: slot %d has not been reported finished "
+                                     "by nwb_pool_query_end", s);
+    if (state)
+        NWB_PCU(cudaMemcpy2DAsync(state, sizeof(double) * h.npts, h.dev.u[h.dev.par], sizeof(double) * h.stride,
+                                  sizeof(double) * h.npts, 6, cudaMemcpyDeviceToHost, p->st));
+    if (energy)
+        NWB_PCU(cudaMemcpyAsync(energy, h.dev.energy, sizeof(double) * (h.nsteps + 1), cudaMemcpyDeviceToHost,
+                                p->st));
+    if (probes && h.nprobes)
+        NWB_PCU(cudaMemcpyAsync(probes, h.dev.probes, sizeof(double) * 6 * h.nprobes * (h.nsteps + 1),
+                                cudaMemcpyDeviceToHost, p->st));
+    return NWB_OK;
+}
+
 nwb_status nwb_pool_results(nwb_pool* p, int s, double* state, double* energy, double* probes) {
     if (!p || s < 0 || s >= p->max_slots) return set_error(NWB_EINVAL, "nwb_pool_results: bad argument");
     SlotHost& h = p->slots[s];
@@ -644,7 +798,8 @@ nwb_status nwb_pool_results(nwb_pool* p, int s, double* state, double* energy, d
 nwb_status nwb_pool_remove(nwb_pool* p, int s) {
     if (!p || s < 0 || s >= p->max_slots) return set_error(NWB_EINVAL, "nwb_pool_remove: bad argument");
     if (!p->slots[s].used) return set_error(NWB_ENOTFOUND, "nwb_pool_remove: slot %d is free", s);
-    NWB_PCU(cudaStreamSynchronize(p->st));
+    // no host wait: the zeroed record and any later admission into the freed ranges
+    // are queued after the steps (and result copies) already in flight
     p->release_slot(s);
     nwb_status r = p->write_slot(s);  // zeroed descriptor: inactive, no buffers
     p->work_dirty = true;
@@ -745,6 +900,9 @@ nwb_status nwb_pool_destroy(nwb_pool* p) {
         if (p->join_ev[N]) cudaEventDestroy(p->join_ev[N]);
     }
     if (p->fork_ev) cudaEventDestroy(p->fork_ev);
+    if (p->snap_ev) cudaEventDestroy(p->snap_ev);
+    if (p->h_snap) cudaFreeHost(p->h_snap);
+    p->stage.destroy();
     if (p->st) cudaStreamDestroy(p->st);
     delete p;
     return NWB_OK;

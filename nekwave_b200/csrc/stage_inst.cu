@@ -4,6 +4,7 @@
 #include "stage_mma.cuh"
 #include "stage_pipe.cuh"
 #include "stage_dmma.cuh"
+#include "stage_bulk.cuh"
 #include "stage_variants.h"
 
 #ifndef NWB_N
@@ -27,8 +28,8 @@ struct Shape {
 constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 #undef NWB_X
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
-// FP64 tensor-core shapes: axis-aligned class, FP64 only
-constexpr bool fp64_only(int alg) { return alg == 1 || alg == 200 || alg == 201; }
+// FP64 tensor-core shapes and the bulk-copy form: axis-aligned class, FP64 only
+constexpr bool fp64_only(int alg) { return alg == 1 || alg == 200 || alg == 201 || alg >= 1000; }
 constexpr int count_simt() {
     int n = 0;
     for (int i = 0; i < kNumShapes; ++i) n += !fp64_only(kShapes[i].alg);
@@ -78,6 +79,16 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                     return launch2<NWB_N, GEO, F32, v.ks, v.epb, v.minb, (fl & 1) != 0, (fl & 2) != 0,
                                    (fl & 4) != 0, cd, (fl & 16) != 0, (fl & 32) != 0,
                                    (fl & 64) != 0>(p, st, cfg);
+                else
+                    return cudaErrorInvalidValue;
+            } else if constexpr (v.alg >= 1000) {
+                // the bulk-copy one-tile form (stage_bulk.cuh), second-family flags
+                // ALG - 1000: 2 SPLIT (required), 8 CONSTD, 16 EARLY, 32 KSM, 64 DSMEM
+                constexpr int fl = v.alg - 1000;
+                static_assert((fl & 2) != 0 && v.ks == 2 && fl < 128, "the field split");
+                if constexpr (GEO == GEO_BOX && !F32)
+                    return launch_bulk<NWB_N, GEO, v.ks, v.epb, v.minb, (fl & 8) != 0, (fl & 64) != 0,
+                                       (fl & 32) != 0, (fl & 16) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == kFirstGeneral) {

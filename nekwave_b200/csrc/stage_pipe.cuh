@@ -240,12 +240,13 @@ struct FaceGather {
 // Fill a FaceGather.  FROM_SMEM: the tile is resident (connections from sc,
 // neighbours inside the tile from su); otherwise only global memory is read, so
 // it may run while the tile's copies are still in flight.
-template <int N, int GEO, int KS, int EPB, bool PAD, bool FROM_SMEM, int FPT>
+template <int N, int GEO, int KS, int EPB, bool PAD, bool FROM_SMEM, int FPT, int CSX = 0>
 __device__ __forceinline__ void gather2(const StageParams& P, const int e0, const double* su,
                                         const int* sc, const int tid, FaceGather<FPT>& G) {
     constexpr int N2 = N * N, N3 = N2 * N;
     constexpr int TPE = KS * N2;
-    constexpr int CS = EPB * (PAD ? N2 * (N + 1) : N3);
+    // component stride of the shared tile (CSX: a tile with slack between components)
+    constexpr int CS = CSX ? CSX : EPB * (PAD ? N2 * (N + 1) : N3);
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
     const int nvalid = min(EPB, P.nelt - e0);
@@ -299,7 +300,8 @@ __device__ __forceinline__ void gather2(const StageParams& P, const int e0, cons
                 if constexpr (FROM_SMEM) in_tile = eB >= e0 && eB < e0 + nvalid;
                 if (in_tile) {
                     const int el = eB - e0;
-                    const int sidx = el * (CS / EPB) + pidx<N, PAD>(static_cast<int>(vB - static_cast<long long>(eB) * N3));
+                    constexpr int EN3 = PAD ? N2 * (N + 1) : N3;  // element stride in the tile
+                    const int sidx = el * EN3 + pidx<N, PAD>(static_cast<int>(vB - static_cast<long long>(eB) * N3));
 #pragma unroll
                     for (int c = 0; c < 6; ++c) G.nb[q][c] = su[c * CS + sidx];
                 } else {
@@ -324,7 +326,7 @@ __host__ __device__ constexpr int face_points_per_thread() {
 // values of all of a thread's points requested first (unless EARLY already did),
 // then the numerical flux of each point times its lift, stored in sflux
 // [team][face][component][point].  The caller synchronises afterwards.
-template <int N, int GEO, bool F32, int KS, int EPB, bool PAD, bool EARLY>
+template <int N, int GEO, bool F32, int KS, int EPB, bool PAD, bool EARLY, int CSX = 0>
 __device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, const double* su,
                                             const ElemGeo* sg, const int* sc, double* sflux,
                                             const int tid,
@@ -334,14 +336,14 @@ __device__ __forceinline__ void face_phase2(const StageParams& P, const int e0, 
     constexpr int RP = PAD ? N + 1 : N;
     constexpr int EN3 = RP * N * N;
     constexpr int TPE = KS * N2;
-    constexpr int CS = EPB * EN3;
+    constexpr int CS = CSX ? CSX : EPB * EN3;
     constexpr int FPT = face_points_per_thread<N, KS>();
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
     const int nvalid = min(EPB, P.nelt - e0);
     const int e = e0 + team;
     const bool active = team < nvalid;
-    if constexpr (!EARLY) gather2<N, GEO, KS, EPB, PAD, true>(P, e0, su, sc, tid, G);
+    if constexpr (!EARLY) gather2<N, GEO, KS, EPB, PAD, true, FPT, CSX>(P, e0, su, sc, tid, G);
     if (active) {
         const double* U = su + team * EN3;
 #pragma unroll
@@ -449,13 +451,20 @@ __device__ __forceinline__ void face_phase_global(const StageParams& P, const in
     }
 }
 
+// Barrier of the threads that share one tile (the whole block in every form here).
+struct CtaBar {
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
 template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
-          bool EARLY = false, bool FACEDONE = false, bool DSMEM = false>
+          bool EARLY = false, bool FACEDONE = false, bool DSMEM = false, class Bar = CtaBar,
+          int CSX = 0, bool KSM = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
                                          FaceGather<face_points_per_thread<N, KS>()>& G,
-                                         const double* __restrict__ Dc = nullptr) {
+                                         const double* __restrict__ Dc = nullptr, Bar bar = Bar(),
+                                         const double* sk = nullptr) {
     using TC = typename std::conditional<F32, float, double>::type;
     constexpr int N2 = N * N, N3 = N2 * N;
     constexpr int RP = PAD ? N + 1 : N;              // row pitch in shared memory
@@ -464,7 +473,9 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     constexpr int TPE = KS * N2;
     constexpr int NT = EPB * TPE;
     constexpr int KPT = (N + KS - 1) / KS;
-    constexpr int CS = EPB * EN3;
+    constexpr int CS = CSX ? CSX : EPB * EN3;
+    static_assert(CSX == 0 || !F32, "tiles with slack: FP64 only");
+    static_assert(!KSM || (!PAD && !F32), "k in shared memory: unpadded FP64 tiles");
     static_assert(!SPLIT || KS == 1 || KS == 2, "the field split: one or two threads per column");
     static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
 
@@ -557,8 +568,9 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     }
 
     // ---- face phase (unless the caller ran it from global memory) -------------------
-    if constexpr (!FACEDONE) face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY>(P, e0, su, sg, sc, sflux, tid, G);
-    __syncthreads();
+    if constexpr (!FACEDONE)
+        face_phase2<N, GEO, F32, KS, EPB, PAD, EARLY, CSX>(P, e0, su, sg, sc, sflux, tid, G);
+    bar.sync();
 
     if constexpr (F32 && GEO != GEO_NODAL) {
         // (c) FP32-bulk deviations w = u - L: each thread takes its own node column
@@ -581,7 +593,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 }
             }
         }
-        __syncthreads();
+        bar.sync();
     }
 
     // ---- column phase: volume curl + face terms + LSRK update ------------------
@@ -624,9 +636,12 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
         // latency overlaps the sums (B200: 3-5% faster at N = 7, 9; the rolled loop
         // is faster without it)
         double knext[3];
+        // KSM: k staged in shared memory with the tile's layout (unpadded)
+        const double* Kf = KSM ? sk + team * EN3 : nullptr;
         if constexpr (CONSTD) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) knext[c] = __ldcg(P.k + (dst + c) * S + ebase + i + N * j);
+            for (int c = 0; c < 3; ++c)
+                knext[c] = KSM ? Kf[(dst + c) * CS + i + RP * j] : __ldcg(P.k + (dst + c) * S + ebase + i + N * j);
         }
 #pragma unroll (CONSTD ? N : 1)
         for (int k = 0; k < N; ++k) {
@@ -639,11 +654,13 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 for (int c = 0; c < 3; ++c) kold[c] = knext[c];
                 if (k + 1 < N) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) knext[c] = __ldcg(P.k + (dst + c) * S + g + N2);
+                    for (int c = 0; c < 3; ++c)
+                        knext[c] = KSM ? Kf[(dst + c) * CS + ms + PP] : __ldcg(P.k + (dst + c) * S + g + N2);
                 }
             } else {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) kold[c] = __ldcg(P.k + (dst + c) * S + g);
+                for (int c = 0; c < 3; ++c)
+                    kold[c] = KSM ? Kf[(dst + c) * CS + ms] : __ldcg(P.k + (dst + c) * S + g);
             }
             double rhs[3];
             if constexpr (GEO == GEO_BOX) {
@@ -723,7 +740,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
             const long long g = ebase + mn;
             double kold[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) kold[c] = __ldcg(P.k + c * S + g);
+            for (int c = 0; c < 6; ++c)
+                kold[c] = KSM ? sk[c * CS + team * EN3 + ms] : __ldcg(P.k + c * S + g);
             double rhs[6];
             if constexpr (GEO == GEO_BOX) {
                 TC Hz_r = 0, Hy_r = 0, Ez_r = 0, Ey_r = 0;

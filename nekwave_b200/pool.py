@@ -67,6 +67,23 @@ def locate_probes(mesh, points):
     return np.array(elems, dtype=np.int32), np.array(weights, dtype=np.float64).reshape(-1)
 
 
+def box_probes(N, nel, lo, hi, points):
+    """ProbeManager::init (src/probe.cpp:33-96) on a box mesh given by its
+    parameters, through libnwb's locator (nwb_box_probes, the one the pool uses):
+    (element offsets e*N^3 [P], tensor weights [P, N^3])."""
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+    P = pts.shape[0]
+    elem = np.zeros(max(P, 1), np.int32)
+    w1d = np.zeros(max(P, 1) * 3 * N)
+    check(_lib.lib().nwb_box_probes(int(N), int(nel[0]), int(nel[1]), int(nel[2]), float(lo[0]),
+                                    float(hi[0]), float(lo[1]), float(hi[1]), float(lo[2]),
+                                    float(hi[2]), P, dptr(pts), iptr(elem), dptr(w1d)))
+    w1d = w1d[:P * 3 * N].reshape(P, 3, N)
+    # tensor weight of node i + N (j + N k): w_r[i] w_s[j] w_t[k] (src/probe.cpp order)
+    w = (w1d[:, 0, None, None, :] * w1d[:, 1, None, :, None]) * w1d[:, 2, :, None, None]
+    return elem[:P].astype(np.int64) * N ** 3, w.reshape(P, N ** 3)
+
+
 class CavityPool:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 256, precision: str = "fp64"):
         self._h = C.c_void_p()
@@ -137,6 +154,33 @@ class CavityPool:
         dn = np.zeros(self.max_slots, np.int32)
         check(_lib.lib().nwb_pool_query(self._h, iptr(st), iptr(dn), self.max_slots))
         return st, dn
+
+    def query_begin(self) -> None:
+        """Queue a snapshot of every slot's status behind the work already queued
+        (nwb_pool_query_begin); query_end() returns it."""
+        check(_lib.lib().nwb_pool_query_begin(self._h))
+
+    def query_end(self):
+        """(status, steps done) as of the last query_begin(), waiting only for that
+        snapshot: steps queued after it keep running."""
+        st = np.zeros(self.max_slots, np.int32)
+        dn = np.zeros(self.max_slots, np.int32)
+        check(_lib.lib().nwb_pool_query_end(self._h, iptr(st), iptr(dn), self.max_slots))
+        return st, dn
+
+    def results_async(self, slot: int) -> dict:
+        """Queue the copies of a finished slot's energy history and probe traces into
+        pinned host buffers and return them at once; they hold the values once a
+        later query_end() (or sync()) has returned.  The slot may be removed
+        right away."""
+        import torch  # pinned host buffers (plumbing)
+        m = self._meta[slot]
+        ne = m["nsteps"] + 1
+        e = torch.empty(ne, dtype=torch.float64, pin_memory=True).numpy()
+        p = torch.empty(ne * max(m["nprobes"], 1) * 6, dtype=torch.float64, pin_memory=True).numpy()
+        check(_lib.lib().nwb_pool_results_async(self._h, int(slot), C.cast(None, _lib._D), dptr(e),
+                                                dptr(p)))
+        return {"energy": e, "probes": p[:ne * m["nprobes"] * 6].reshape(ne, m["nprobes"], 6)}
 
     def results(self, slot: int, state=True, energy=True, probes=True) -> dict:
         m = self._meta[slot]

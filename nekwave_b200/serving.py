@@ -39,6 +39,8 @@ class Result:
     finished: float
     probes: np.ndarray       # [nsteps+1, 8, 6]
     energy: np.ndarray       # [nsteps+1] (NaN where not recorded)
+    retired: float = 0.0     # when the server saw it finished and freed its slot
+                             # (its results reach the host by `finished`)
 
     @property
     def latency(self):
@@ -70,15 +72,24 @@ class Server:
     def run(self, requests, time_scale: float = 1.0, log=None):
         """Serve the stream in real time (arrivals replayed at time_scale x the
         request timestamps).  Returns the results in request order and the
-        wall time of the whole run."""
+        wall time of the whole run.
+
+        The host never waits for the GPU to drain: each round queues the next
+        chunk of steps first and only then waits for the status snapshot queued
+        after the previous chunk (nwb_pool_query_begin/end), so the GPU works
+        on the new chunk while the host retires finished requests (their
+        results copied asynchronously, complete by the next snapshot) and
+        admits new ones (queued behind the running chunk)."""
         pending = []
         arrivals = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
         nxt = 0
         running = {}            # slot -> (request index, admit time)
+        fetching = {}           # request index -> (admit time, result buffers in flight)
+        snapshot = False        # a status snapshot is queued
         results = [None] * len(requests)
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
-        while nxt < len(arrivals) or pending or running:
+        while nxt < len(arrivals) or pending or running or fetching:
             t = now()
             while nxt < len(arrivals) and requests[arrivals[nxt]].arrival * time_scale <= t:
                 pending.append(arrivals[nxt])
@@ -98,31 +109,43 @@ class Server:
                 pending.pop(0)
                 running[s] = (i, now())
                 resident += requests[i].npts
-            if not running:
+            if not running and not snapshot:
                 if nxt < len(arrivals):          # idle until the next arrival
                     wait = requests[arrivals[nxt]].arrival * time_scale - now()
                     if wait > 0:
                         time.sleep(min(wait, 0.05))
                 continue
-            self.pool.step(self.chunk)
-            status, _ = self.pool.query()
-            for s in [s for s in running if status[s] == FINISHED]:
-                i, ta = running.pop(s)
-                r = self.pool.results(s, state=False)
-                results[i] = Result(i, requests[i].arrival * time_scale, ta, now(), r["probes"],
-                                    r["energy"])
-                self.pool.remove(s)
-                if log:
-                    log(results[i])
+            if running:
+                self.pool.step(self.chunk)
+            if snapshot:
+                status, _ = self.pool.query_end()
+                # result copies queued before that snapshot have landed
+                for i, (ta, tr, r) in fetching.items():
+                    results[i] = Result(i, requests[i].arrival * time_scale, ta, now(), r["probes"],
+                                        r["energy"], retired=tr)
+                    if log:
+                        log(results[i])
+                fetching = {}
+                for s in [s for s in running if status[s] == FINISHED]:
+                    i, ta = running.pop(s)
+                    fetching[i] = (ta, now(), self.pool.results_async(s))
+                    self.pool.remove(s)
+            snapshot = bool(running or fetching)
+            if snapshot:
+                self.pool.query_begin()
         return results, now()
 
 
-def serve_serial(requests, precision="fp64", time_scale: float = 1.0):
+def serve_serial(requests, precision="fp64", time_scale: float = 1.0, energy_every: int = 10):
     """The same stream served one request at a time with the single-mesh solver,
-    the reference's execution model (box solver built per request, device initial
-    state, nsteps steps from a CUDA graph, final energy read back).  It records
-    no per-step probes or energy, which only favours it."""
+    the reference's execution model (Case::simulate, src/case.cpp:562-655: one
+    solve per process, a step at a time, probes recorded after every step and the
+    energy every output step).  Box solver built per request, device initial
+    state; the probes (ProbeManager::record) and the energy are evaluated on the
+    device and only their values are read back, which spares it the reference's
+    full per-step download."""
     from . import DgSolver
+    from .pool import box_probes
     order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
     results = [None] * len(requests)
     t0 = time.perf_counter()
@@ -135,11 +158,24 @@ def serve_serial(requests, precision="fp64", time_scale: float = 1.0):
         s = DgSolver(precision)
         s.initializeBox(req.N, req.nel, req.lo, req.hi, req.c0, periodic=req.periodic)
         s.initPulse(req.pulses)
-        s.steps(req.dt, req.nsteps)
-        energy = np.array([s.energy()])
+        np_ = len(req.probes)
+        if np_:
+            off, w = box_probes(req.N, req.nel, req.lo, req.hi, req.probes)
+            s.probeSetup(off, w)
+        probes = np.zeros((req.nsteps + 1, np_, 6))
+        energy = np.full(req.nsteps + 1, np.nan)
+        energy[0] = s.energy()
+        if np_:
+            probes[0] = s.probeRead()
+        for n in range(1, req.nsteps + 1):
+            s.step(req.dt, 0.0)
+            if np_:
+                probes[n] = s.probeRead()
+            if n % energy_every == 0 or n == req.nsteps:
+                energy[n] = s.energy()
         s.finalize()
-        results[i] = Result(i, req.arrival * time_scale, ta, time.perf_counter() - t0,
-                            np.zeros((0, 0, 6)), energy)
+        tf = time.perf_counter() - t0
+        results[i] = Result(i, req.arrival * time_scale, ta, tf, probes, energy, retired=tf)
     return results, time.perf_counter() - t0
 
 

@@ -51,9 +51,22 @@ class FakePool:
             done[s] = d
         return status, done
 
+    def query_begin(self):
+        # the snapshot reflects every step queued so far (the stand-in steps at once)
+        self._snap = self.query()
+
+    def query_end(self):
+        snap, self._snap = self._snap, None
+        assert snap is not None, "query_end without query_begin"
+        return snap
+
     def results(self, slot, state=True, energy=True, probes=True):
         nsteps = self.slots[slot][1]
         return {"probes": np.zeros((nsteps + 1, 8, 6)), "energy": np.zeros(nsteps + 1)}
+
+    def results_async(self, slot):
+        assert self.slots[slot][2] >= self.slots[slot][1], "results of an unfinished cavity"
+        return self.results(slot)
 
     def remove(self, slot):
         del self.slots[slot]
