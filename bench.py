@@ -87,6 +87,13 @@ def parse():
     p.add_argument("--rates", type=str, default="0.5,1,2",
                    help="serve: arrival rates as multiples of the measured serial service rate")
     p.add_argument("--requests", type=int, default=24, help="serve: requests per rate")
+    p.add_argument("--policies", type=str, default="fifo,sjf", help="serve: admission policies")
+    p.add_argument("--serial-rates", type=str, default=None,
+                   help="serve: rates (multiples) at which the serial path is run (default: --rates; "
+                        "'none' for none)")
+    p.add_argument("--serial-rate-per-s", type=float, default=0.0,
+                   help="serve: the serial service rate (solves/s) to scale the arrivals by, "
+                        "instead of measuring it (lets a sweep be split over runs)")
     p.add_argument("--accuracy-steps", type=int, default=0,
                    help="c2: also run FP64 and FP32-bulk this many steps from the same initial "
                         "state and report the relative L2 error and energy drift")
@@ -186,6 +193,18 @@ def profiled_traffic(N):
         if int(d.get("N", 8)) == N:
             return d
     return None
+
+
+def pool_traffic(seed):
+    """DRAM bytes of one pool stage (all per-N kernels) on the 256-cavity workload of
+    seed 0, from the committed ncu summary (pool_step_traffic.json), or None."""
+    if seed != 0:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "pool_step_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_stage"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 # ---- CPU baseline: the reference's own implementation on the host cores ---------------
@@ -334,8 +353,10 @@ def run_batch(args, rank, world):
                                sum(c.npts for c in inst) * 48 / 1e9)),
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "batch_stage_kernel (+diag, epilogue)"},
+                         "frac": achieved / peak, "traffic": pool_traffic(seed=args.seed + rank),
+                         "peak_source": peak_kind,
+                         "kernel": "one stage: the per-N stage kernels of every N present",
+                         "per_unit": "32 B per DOF-stage x 6 x nodes (all cavities) per stage"},
             "serial_fp64_single_mesh": {"value": serial, "unit": METRIC,
                                         "sample": "first 48 instances solved one at a time with "
                                                   "the single-mesh FP64 solver (CUDA graph per step)",
@@ -354,17 +375,21 @@ def run_serve(args, rank, world):
     n = args.requests
     # serial service rate: the serial path's GDOF-stage/s on a few requests over the
     # mean work of a request of this distribution (2000 samples, no GPU work)
-    calib = serving_requests(4, 1e9, seed=args.seed + 1000)
-    _, cal_wall = serve_serial(calib, precision="fp64")
-    serial_rate = sum(c.dof_stages for c in calib) / cal_wall
     mean_work = float(np.mean([c.dof_stages for c in serving_requests(2000, 1.0, seed=args.seed + 7)]))
-    mu = serial_rate / mean_work
+    if args.serial_rate_per_s > 0:
+        mu = args.serial_rate_per_s
+        serial_rate = mu * mean_work
+    else:
+        calib = serving_requests(4, 1e9, seed=args.seed + 1000)
+        _, cal_wall = serve_serial(calib, precision="fp64")
+        serial_rate = sum(c.dof_stages for c in calib) / cal_wall
+        mu = serial_rate / mean_work
     rows = []
     budget = int(float(os.environ.get("NWB_SERVE_BUDGET_GB", "100")) * (1 << 30))
     base = serving_requests(n, 1.0, seed=args.seed + 100)  # one request set, arrivals at rate 1/s
     for mult in [float(x) for x in args.rates.split(",")]:
         reqs = [dataclasses.replace(r, arrival=r.arrival / (mult * mu)) for r in base]
-        for policy in ("fifo", "sjf"):
+        for policy in [x for x in args.policies.split(",") if x]:
             srv = Server(budget, max_slots=512, precision=args.precision, policy=policy)
             res, wall = srv.run(reqs)
             srv.close()
@@ -374,13 +399,14 @@ def run_serve(args, rank, world):
                              mean_s=st["mean"],
                              gdof_stage_per_s=sum(r.dof_stages for r in reqs) / wall / 1e9))
     serial = []
-    for mult in [float(x) for x in args.rates.split(",")]:
+    srates = args.rates if args.serial_rates is None else args.serial_rates
+    for mult in ([] if srates == "none" else [float(x) for x in srates.split(",")]):
         serial_reqs = [dataclasses.replace(r, arrival=r.arrival / (mult * mu)) for r in base]
         sres, swall = serve_serial(serial_reqs, precision="fp64")
         sst = latency_stats(sres)
         serial.append(dict(rate_multiple=mult, rate_per_s=mult * mu, solves_per_s=n / swall,
                            p50_s=sst["p50"], p99_s=sst["p99"], mean_s=sst["mean"]))
-    best = max(rows, key=lambda r: r["solves_per_s"])
+    best = max(rows, key=lambda r: r["solves_per_s"]) if rows else {"solves_per_s": None}
     return {"metric": "solves/s", "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": world,
             "steps": n, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -391,7 +417,10 @@ def run_serve(args, rank, world):
                            mean_request_gdof_stage=mean_work / 1e9, max_elements_per_dir=48,
                            points_per_dir="4..9", budget_gb=budget / (1 << 30)),
             "serving": rows,
-            "serial_fp64": serial}
+            "serial_fp64": serial,
+            "serial_pattern": "one request at a time with the single-mesh FP64 solver, a step at a "
+                              "time, the 8 probes read after every step and the energy every 10 "
+                              "steps (the reference's Case::simulate loop, diagnostics on the device)"}
 
 
 def main():

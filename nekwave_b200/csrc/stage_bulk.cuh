@@ -177,18 +177,40 @@ __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, un
         P, e0, su, sg, sc, sD, sflux, nullptr, tid, G, Dc, CtaBar(), sk);
 }
 
-template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY>
+// Tile taken by block b.  ZCOL on a structured box whose rows hold whole tiles:
+// blocks walk the tiles of one (x-tile, y) column through every z before the next
+// column, so an element's z-neighbours (nx*ny elements away in memory) are
+// loaded by blocks that run at about the same time and their shared face planes
+// come from L2 instead of a second DRAM read.  Otherwise tiles in memory order.
+template <int EPB, bool ZCOL>
+__device__ __forceinline__ int bulk_tile_index(const StageParams& P, int b) {
+    if constexpr (ZCOL) {
+        const int nx = P.snel[0], ny = P.snel[1], nz = P.snel[2];
+        if (nx > 0 && nx % EPB == 0) {
+            const int col = b / nz, ez = b - col * nz;
+            const int ntx = nx / EPB;
+            const int ey = col / ntx, xt = col - ey * ntx;
+            return xt + ntx * (ey + ny * ez);
+        }
+    }
+    return b;
+}
+
+template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
+          bool ZCOL>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage_bulk_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY>(P, blockIdx.x * EPB, smem, threadIdx.x, P.Dc);
+    const int t = bulk_tile_index<EPB, ZCOL>(P, blockIdx.x);
+    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY>(P, t * EPB, smem, threadIdx.x, P.Dc);
 }
 
-template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY>
+template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
+          bool ZCOL>
 cudaError_t launch_bulk(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int threads = EPB * KS * N * N;
-    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY>;
+    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, L::total, KSM ? 1 : 0, MINB};
     static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
     if (cudaError_t e = set_smem_once(kern, L::total, attr_set); e != cudaSuccess) return e;

@@ -56,6 +56,11 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
+// FP32-bulk, affine classes: an element runs the FP64 column arithmetic when the
+// largest deviation of its tile from the per-element linear fit exceeds this
+// fraction of the largest deviation from its centre value (in any component).
+constexpr float kFp64Fallback = 0.125f;
+
 // Shared-memory index of local node n = i + N j + N^2 k of a tile (element-major).
 template <int N, bool PAD>
 __device__ __forceinline__ int pidx(int n) {
@@ -79,9 +84,12 @@ struct Layout2 {
     static constexpr int flux = D + align16(N2 * 8);
     static constexpr int uc = flux + EPB * 36 * N2 * 8;
     // FP32-bulk: the tile's deviations [6][CS] floats, then per element the linear
-    // fit ([6][4]: centre value, slopes along r, s, t) and its curl ([6]), then zl
+    // fit ([6][4]: centre value, slopes along r, s, t) and its curl ([6]), then zl,
+    // then per element the largest deviation and variation (FP64 fallback test)
     static constexpr int LIN = 30;
-    static constexpr int total = uc + (F32 ? align16(6 * CS * 4) + align16((EPB * LIN + 10) * 8) : 0);
+    static constexpr int total = uc + (F32 ? align16(6 * CS * 4) + align16((EPB * LIN + 10) * 8) +
+                                                 align16(EPB * 2 * 4)
+                                           : 0);
     static_assert(tile % 16 == 0 && geo_b % 16 == 0, "16-byte aligned buffers");
 };
 
@@ -494,6 +502,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     // FP32-bulk, affine classes: per element the linear fit's curl, added in FP64
     constexpr int LIN = 30;
     const double* s_lin = nullptr;
+    unsigned* s_fb = nullptr;  // per element: bits of the largest |w| and |u - centre|
     if constexpr (F32 && GEO == GEO_NODAL) {
         // FP32 copy of the tile as deviations from the element's centre node: the
         // derivatives are unchanged (rows of D sum to zero) and the rounding error
@@ -520,6 +529,8 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
         constexpr int lin_off = (6 * CS * 4 + 15) & ~15;  // after the deviations (Layout2::uc)
         double* lin = reinterpret_cast<double*>(smem_uc + lin_off);
         double* szl = lin + EPB * LIN;
+        s_fb = reinterpret_cast<unsigned*>(szl + 10);
+        if (tid < 2 * EPB) s_fb[tid] = 0u;  // formed in (c), after the face phase's barrier
         constexpr int ic = N / 2;
         const double inv = 1.0 / (P.zl[N - 1] - P.zl[0]);
         const int nlin = tid < NT ? nvalid * 6 : 0;
@@ -581,6 +592,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
             const double* szl = s_lin + EPB * LIN;
             constexpr int ic = N / 2;
             const double zi = szl[i] - szl[ic], zj = szl[j] - szl[ic];
+            float wmax = 0.f, vmax = 0.f;
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
                 const double* Lc = s_lin + team * LIN + 4 * c;
@@ -589,9 +601,15 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 const int col = c * CS + team * EN3 + i + RP * j;
                 for (int k = h; k < N; k += KS) {
                     const double Lv = base + at * (szl[k] - szl[ic]);
-                    w[col + PP * k] = static_cast<float>(su[col + PP * k] - Lv);
+                    const float wv = static_cast<float>(su[col + PP * k] - Lv);
+                    w[col + PP * k] = wv;
+                    wmax = fmaxf(wmax, fabsf(wv));
+                    vmax = fmaxf(vmax, fabsf(static_cast<float>(su[col + PP * k] - Lc[0])));
                 }
             }
+            // non-negative floats order as their bit patterns
+            atomicMax(s_fb + 2 * team, __float_as_uint(wmax));
+            atomicMax(s_fb + 2 * team + 1, __float_as_uint(vmax));
         }
         bar.sync();
     }
@@ -616,6 +634,24 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     const long long ebase = static_cast<long long>(e) * N3;
 
     if constexpr (SPLIT) {
+        // FP32-bulk: an element whose deviations from its linear fit are not small
+        // against its variation (a field resolved within one or two elements, where
+        // the fit removes little) runs the FP64 arithmetic on u itself: its FP32
+        // rounding would not shrink with the deviations there.
+        bool fb64 = false;
+        if constexpr (F32 && GEO != GEO_NODAL)
+            fb64 = __uint_as_float(s_fb[2 * team]) > kFp64Fallback * __uint_as_float(s_fb[2 * team + 1]);
+        // the column work in arithmetic type TX (TC, or FP64 for a fallback element)
+        auto columns = [&](auto zero) {
+        using TX = decltype(zero);
+        constexpr bool SAME = std::is_same<TX, TC>::value;
+        const TX* ubase;
+        if constexpr (SAME) ubase = U;
+        else ubase = Uf;
+        auto met = [&](int c) -> TX {
+            if constexpr (SAME) return m_[c];
+            else return static_cast<TX>(sg[team].met[c]);
+        };
         // field hf = 0: E residual from V = H (+curl H); hf = 1: H residual from V = E
         // (-curl E).  KS = 2: thread h takes field h; KS = 1: one thread takes both,
         // one after the other, with the same arithmetic per node.
@@ -624,9 +660,9 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
         const int src = hf == 0 ? 3 : 0;
         const int dst = 3 - src;
         const double sgn = hf == 0 ? 1.0 : -1.0;
-        const TC* V = U + src * CS;
+        const TX* V = ubase + src * CS;
         constexpr int NC = GEO == GEO_BOX ? 2 : 3;  // components differentiated along t
-        TC col[NC][N];
+        TX col[NC][N];
 #pragma unroll
         for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -664,29 +700,29 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
             }
             double rhs[3];
             if constexpr (GEO == GEO_BOX) {
-                TC Vz_r = 0, Vy_r = 0, Vz_s = 0, Vx_s = 0, Vy_t = 0, Vx_t = 0;
+                TX Vz_r = 0, Vy_r = 0, Vz_s = 0, Vx_s = 0, Vy_t = 0, Vx_t = 0;
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
-                    const TC dr = DSMEM ? static_cast<TC>(sD[i + l * N]) : Dr[l];
-                    const TC ds = DSMEM ? static_cast<TC>(sD[j + l * N]) : Ds[l];
-                    const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
+                    const TX dr = (DSMEM || !SAME) ? static_cast<TX>(sD[i + l * N]) : static_cast<TX>(Dr[l]);
+                    const TX ds = (DSMEM || !SAME) ? static_cast<TX>(sD[j + l * N]) : static_cast<TX>(Ds[l]);
+                    const TX dt = CONSTD ? static_cast<TX>(Dc[k + l * N]) : static_cast<TX>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
                     Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
                     Vz_s += ds * V[2 * CS + is]; Vx_s += ds * V[0 * CS + is];
                     Vy_t += dt * col[1][l]; Vx_t += dt * col[0][l];
                 }
-                const TC rx = m_[0], sy = m_[4], tz = m_[8];
+                const TX rx = met(0), sy = met(4), tz = met(8);
                 rhs[0] = sgn * static_cast<double>(sy * Vz_s - tz * Vy_t);
                 rhs[1] = sgn * static_cast<double>(tz * Vx_t - rx * Vz_r);
                 rhs[2] = sgn * static_cast<double>(rx * Vy_r - sy * Vx_s);
             } else {
-                TC dr_[3] = {0, 0, 0}, ds_[3] = {0, 0, 0}, dt_[3] = {0, 0, 0};
+                TX dr_[3] = {0, 0, 0}, ds_[3] = {0, 0, 0}, dt_[3] = {0, 0, 0};
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
-                    const TC dr = DSMEM ? static_cast<TC>(sD[i + l * N]) : Dr[l];
-                    const TC ds = DSMEM ? static_cast<TC>(sD[j + l * N]) : Ds[l];
-                    const TC dt = CONSTD ? static_cast<TC>(Dc[k + l * N]) : static_cast<TC>(sD[k + l * N]);
+                    const TX dr = (DSMEM || !SAME) ? static_cast<TX>(sD[i + l * N]) : static_cast<TX>(Dr[l]);
+                    const TX ds = (DSMEM || !SAME) ? static_cast<TX>(sD[j + l * N]) : static_cast<TX>(Ds[l]);
+                    const TX dt = CONSTD ? static_cast<TX>(Dc[k + l * N]) : static_cast<TX>(sD[k + l * N]);
                     const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
 #pragma unroll
@@ -696,26 +732,26 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                         dt_[c] += dt * col[c][l];
                     }
                 }
-                TC rx, sx, tx, ry, sy, ty, rz, sz, tz;
+                TX rx, sx, tx, ry, sy, ty, rz, sz, tz;
                 if constexpr (GEO == GEO_NODAL) {
-                    rx = static_cast<TC>(P.met_n[0 * S + g]); sx = static_cast<TC>(P.met_n[1 * S + g]);
-                    tx = static_cast<TC>(P.met_n[2 * S + g]); ry = static_cast<TC>(P.met_n[3 * S + g]);
-                    sy = static_cast<TC>(P.met_n[4 * S + g]); ty = static_cast<TC>(P.met_n[5 * S + g]);
-                    rz = static_cast<TC>(P.met_n[6 * S + g]); sz = static_cast<TC>(P.met_n[7 * S + g]);
-                    tz = static_cast<TC>(P.met_n[8 * S + g]);
+                    rx = static_cast<TX>(P.met_n[0 * S + g]); sx = static_cast<TX>(P.met_n[1 * S + g]);
+                    tx = static_cast<TX>(P.met_n[2 * S + g]); ry = static_cast<TX>(P.met_n[3 * S + g]);
+                    sy = static_cast<TX>(P.met_n[4 * S + g]); ty = static_cast<TX>(P.met_n[5 * S + g]);
+                    rz = static_cast<TX>(P.met_n[6 * S + g]); sz = static_cast<TX>(P.met_n[7 * S + g]);
+                    tz = static_cast<TX>(P.met_n[8 * S + g]);
                 } else {
-                    rx = m_[0]; sx = m_[1]; tx = m_[2]; ry = m_[3]; sy = m_[4];
-                    ty = m_[5]; rz = m_[6]; sz = m_[7]; tz = m_[8];
+                    rx = met(0); sx = met(1); tx = met(2); ry = met(3); sy = met(4);
+                    ty = met(5); rz = met(6); sz = met(7); tz = met(8);
                 }
                 // physical curl, src/device/dg_kernels.cu:140-149
-                const TC c1 = (dr_[2] * ry + ds_[2] * sy + dt_[2] * ty) - (dr_[1] * rz + ds_[1] * sz + dt_[1] * tz);
-                const TC c2 = (dr_[0] * rz + ds_[0] * sz + dt_[0] * tz) - (dr_[2] * rx + ds_[2] * sx + dt_[2] * tx);
-                const TC c3 = (dr_[1] * rx + ds_[1] * sx + dt_[1] * tx) - (dr_[0] * ry + ds_[0] * sy + dt_[0] * ty);
+                const TX c1 = (dr_[2] * ry + ds_[2] * sy + dt_[2] * ty) - (dr_[1] * rz + ds_[1] * sz + dt_[1] * tz);
+                const TX c2 = (dr_[0] * rz + ds_[0] * sz + dt_[0] * tz) - (dr_[2] * rx + ds_[2] * sx + dt_[2] * tx);
+                const TX c3 = (dr_[1] * rx + ds_[1] * sx + dt_[1] * tx) - (dr_[0] * ry + ds_[0] * sy + dt_[0] * ty);
                 rhs[0] = sgn * static_cast<double>(c1);
                 rhs[1] = sgn * static_cast<double>(c2);
                 rhs[2] = sgn * static_cast<double>(c3);
             }
-            if constexpr (F32 && GEO != GEO_NODAL) {
+            if constexpr (F32 && GEO != GEO_NODAL && SAME) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) rhs[c] += s_lin[team * LIN + 24 + dst + c];
             }
@@ -728,6 +764,13 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                 __stcs(P.u_out + (dst + c) * S + g, Uf[(dst + c) * CS + ms] + B * kn);
             }
         }
+        }
+        };
+        if constexpr (F32 && GEO != GEO_NODAL) {
+            if (fb64) columns(0.0);
+            else columns(0.0f);
+        } else {
+            columns(TC(0));
         }
     } else {
         // one plane at a time: the register budget goes to the batched loads

@@ -229,3 +229,34 @@ def test_fp32_bulk_smooth_pulse_within_1e6_and_pool_equals_single(gpu):
     pool.step(ns)
     np.testing.assert_array_equal(pool.results(s)["state"], out["fp32"])
     pool.close()
+
+
+def test_fp32_bulk_meets_1e6_on_the_least_resolved_batch_instances(gpu):
+    """The FP32-bulk gate on the batched workload's hardest cavities: of the 256
+    seeded instances (400 steps each, upwind, PEC), the 12 whose pulse spans the
+    fewest elements, advanced in an FP32-bulk pool and an FP64 pool.  Every
+    instance stays within 1e-6 relative L2 of FP64 (elements whose field departs
+    from linear across the element run the FP64 arithmetic); the errors are
+    recorded (fp32_gate_batch.json)."""
+    from nekwave_b200.workloads import batch_instances
+    from tests.gpu_helpers import record
+    inst = batch_instances(256, seed=0, steps=400)
+
+    def resolution(c):  # pulse width in element sizes, along the coarsest axis
+        return c.pulses[2][4] / max((c.hi[a] - c.lo[a]) / c.nel[a] for a in range(3))
+
+    pick = sorted(inst, key=resolution)[:12]
+    out = {}
+    for prec in ("fp64", "fp32"):
+        pool = CavityPool(8 << 30, max_slots=len(pick), precision=prec)
+        slots = [pool.add_box(c.N, c.nel, c.lo, c.hi, c.c0, c.dt, c.nsteps) for c in pick]
+        for s, c in zip(slots, pick):
+            pool.init_pulse(s, c.pulses)
+        pool.step(400)
+        out[prec] = [pool.results(s, energy=False, probes=False)["state"] for s in slots]
+        pool.close()
+    errs = [rel_l2(a, b) for a, b in zip(out["fp32"], out["fp64"])]
+    record("fp32_gate_batch.json", {"instances": len(pick), "steps": 400,
+                                    "resolution_elements": [resolution(c) for c in pick],
+                                    "N": [c.N for c in pick], "rel_l2": errs, "max": max(errs)})
+    assert max(errs) <= 1e-6, errs
