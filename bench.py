@@ -224,7 +224,7 @@ def _sample_mesh(spec, O):
     return m, O.dxmin(m), O.step, O.threads(), "port"
 
 
-def cpu_reference_rate(seconds_target=12.0, spec=None):
+def cpu_reference_rate(seconds_target=12.0, spec=None, one_core=0.0):
     """Times the reference's RHS + LSRK45 (its kernel bodies compiled for the host,
     oracle/_ref) -- or, if that build is absent, the oracle port -- on a bounded sample
     of the workload: whole LSRK45 steps on an 8x8x8-element sub-box with the same
@@ -242,10 +242,36 @@ def cpu_reference_rate(seconds_target=12.0, spec=None):
     stepper(m, spec["c0"], dt, nsteps, u, k)
     sec = time.perf_counter() - t0
     dof_stage = 6 * m.npts * 5 * nsteps
-    return dict(value=dof_stage / sec / 1e9, unit=METRIC, cores=int(cores), kind=kind,
-                sample=f"{nsteps} LSRK45 steps on an 8x8x8-element sub-box of the workload, "
-                       f"N={spec['N']} ({m.npts} nodes), {sec:.1f} s on {cores} host threads",
-                seconds=sec, steps=nsteps, npts=m.npts)
+    out = dict(value=dof_stage / sec / 1e9, unit=METRIC, cores=int(cores), kind=kind,
+               sample=f"{nsteps} LSRK45 steps on an 8x8x8-element sub-box of the workload, "
+                      f"N={spec['N']} ({m.npts} nodes), {sec:.1f} s on {cores} host threads",
+               seconds=sec, steps=nsteps, npts=m.npts, cpu_model=cpu_model())
+    if one_core and kind == "reference" and cores > 1:
+        # the same sample on one host thread, a bounded number of steps
+        old = O.ref().nwref_set_threads(1)
+        try:
+            n1 = max(1, int(one_core / max(one * cores, 1e-3)))
+            t0 = time.perf_counter()
+            stepper(m, spec["c0"], dt, n1, u, k)
+            s1 = time.perf_counter() - t0
+        finally:
+            O.ref().nwref_set_threads(old)
+        out["one_core"] = dict(value=6 * m.npts * 5 * n1 / s1 / 1e9, unit=METRIC, cores=1,
+                               sample=f"{n1} LSRK45 steps of the same sub-box, {s1:.1f} s on 1 "
+                                      f"host thread")
+    return out
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args, rank, world):
@@ -277,7 +303,7 @@ def run_reference(args, rank, world):
             "config": dict(workload=spec["workload"], N=spec["N"], nel=list(spec["nel"]),
                            flux=spec["flux"], cfl=WORKLOAD["cfl"], sample_nel=[8, 8, 8]),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": int(cores), "kind": kind,
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -559,7 +585,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_rate(spec=spec)
+        cpu = cpu_reference_rate(spec=spec, one_core=6.0)
 
     if dist_on:
         dist.barrier()
@@ -599,7 +625,8 @@ def main():
         if accuracy is not None:
             line["accuracy"] = accuracy
         if cpu is not None:
-            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                          "cpu_model", "one_core") if k in cpu}
         print(json.dumps(line), flush=True)
     solver.finalize()
     if dist_on:

@@ -89,6 +89,8 @@ def ref():
                                  _D, _D, _D, _D, C.c_double, C.c_double, C.c_int, _D, _D,
                                  C.c_int]
         L.nwref_threads.restype = C.c_int
+        L.nwref_set_threads.restype = C.c_int
+        L.nwref_set_threads.argtypes = [C.c_int]
         L.nwref_probe_init.argtypes = [C.c_void_p, C.c_int, _D, C.POINTER(C.c_long), _D]
         _ref = L
     return _ref

@@ -158,4 +158,16 @@ int nwref_threads(void) {
 #endif
 }
 
+// Host threads for the next runs (n >= 1); returns the previous count.
+int nwref_set_threads(int n) {
+#ifdef _OPENMP
+    const int old = omp_get_max_threads();
+    if (n >= 1) omp_set_num_threads(n);
+    return old;
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
 }  // extern "C"
