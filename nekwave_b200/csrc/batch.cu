@@ -255,12 +255,13 @@ template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, M
 
 // FP64 per-N shapes that run the bulk-copy one-tile form (the single-mesh default
 // at these N): k staged in shared memory, CD = t-derivative D from the parameters.
-// EARLY = neighbour traces requested while the tile's copies fly.
-template <int N> struct NBulk { static constexpr bool on = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1; };
-template <> struct NBulk<5> { static constexpr bool on = true, CD = false, EARLY = false; static constexpr int EPB = 2, MINB = 4; };
-template <> struct NBulk<6> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3; };
-template <> struct NBulk<7> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4; };
-template <> struct NBulk<9> { static constexpr bool on = true, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2; };
+// EARLY = neighbour traces requested while the tile's copies fly.  VROW = the
+// r-derivative's node rows read with 16-byte loads.
+template <int N> struct NBulk { static constexpr bool on = false, VROW = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1; };
+template <> struct NBulk<5> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 4; };
+template <> struct NBulk<6> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3; };
+template <> struct NBulk<7> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4; };
+template <> struct NBulk<9> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2; };
 
 template <int N, bool CD>
 __global__ void __launch_bounds__(NBulk<N>::EPB * 2 * N * N, NBulk<N>::MINB)
@@ -271,7 +272,7 @@ batch_bulk_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restric
     const SlotDev& S = slots[w.slot];
     if (!S.active) return;
     const StageParams P = slot_params(S, stage, dry);
-    stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY>(P, w.e0, smem,
+    stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY, NBulk<N>::VROW>(P, w.e0, smem,
                                                                                       threadIdx.x, dp.d);
 }
 

@@ -110,19 +110,73 @@ struct BulkLayout {
     static constexpr int total = flag + 16;
 };
 
+// Thread 0's part of a tile load: the tile's u_in (and with KSM its k; otherwise k's
+// lines are prefetched into L2), geometry and connections as bulk copies that
+// complete on the mbarrier at smem + L::bar, which must be initialised.
+template <int N, int EPB, bool KSM>
+__device__ __forceinline__ void bulk_issue(const StageParams& P, const int e0, unsigned char* smem) {
+    using L = BulkLayout<N, EPB, KSM>;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);
+    const long long S = P.stride;
+    const long long g0 = static_cast<long long>(e0) * L::N3;
+    const int nvalid = min(EPB, P.nelt - e0);
+    const long long a0 = g0 & ~1ll, a1 = (g0 + static_cast<long long>(nvalid) * L::N3 + 1) & ~1ll;
+    const unsigned ub = static_cast<unsigned>((a1 - a0) * 8);
+    const long long c0 = static_cast<long long>(e0) * 6, c1 = c0 + 6 * nvalid;
+    const long long ca0 = c0 & ~3ll, ca1 = (c1 + 3) & ~3ll;
+    const unsigned cb = static_cast<unsigned>((ca1 - ca0) * 4);
+    const unsigned gb = static_cast<unsigned>(nvalid * sizeof(ElemGeo));
+    mbar_arrive_expect_tx(bar, (KSM ? 12 : 6) * ub + gb + cb);
+    double* su = reinterpret_cast<double*>(smem + L::u0);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) bulk_g2s(su + c * L::CSR, P.u_in + c * S + a0, ub, bar);
+    if constexpr (KSM) {
+        double* sk = reinterpret_cast<double*>(smem + L::k0);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) bulk_g2s(sk + c * L::CSR, P.k + c * S + a0, ub, bar);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) bulk_prefetch_l2(P.k + c * S + a0, ub);
+    }
+    bulk_g2s(smem + L::geo0, P.geo + e0, gb, bar);
+    bulk_g2s(smem + L::conn0, P.conn + ca0, cb, bar);
+}
+
+// Every thread's wait for the tile issued by bulk_issue: true when it is resident.
+// On expiry thread 0 records the code, waits once more (bounded) for the copies so
+// that none lands in a finished block, and every thread gets false.
+template <int N, int EPB, bool KSM>
+__device__ __forceinline__ bool bulk_wait_tile(const StageParams& P, unsigned char* smem, const int tid) {
+    using L = BulkLayout<N, EPB, KSM>;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);
+    int* flag = reinterpret_cast<int*>(smem + L::flag);
+    if (tid == 0) *flag = mbar_wait(bar, 0) ? 1 : 0;
+    __syncthreads();
+    if (!*flag) {
+        if (tid == 0) {
+            report(P, kErrTileWait);
+            mbar_wait(bar, 0);
+        }
+        return false;
+    }
+    mbar_test(bar, 0);  // the phase is complete: acquire the tile for this thread
+    return true;
+}
+
 // One tile of the bulk-copy one-tile form, for the single-mesh kernel below and
 // the pool's per-N kernels.  All NT = EPB*KS*N*N threads of the block call it.
 // EARLY: the neighbour traces of the face phase are requested from global memory
 // (through the box structure when there is one) while the tile's copies are in
-// flight.  Dc: D where the t contraction of CONSTD reads it (a parameter copy).
-template <int N, int GEO, int KS, int EPB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY>
+// flight.  VROW: the r-derivative's node rows read with 16-byte loads.  Dc: D where
+// the t contraction of CONSTD reads it (a parameter copy).
+template <int N, int GEO, int KS, int EPB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
+          bool VROW = false>
 __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, unsigned char* smem,
                                           const int tid, const double* Dc) {
     static_assert(GEO != GEO_NODAL, "per-element geometry and connections");
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int NT = EPB * KS * N * N;
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);
-    int* flag = reinterpret_cast<int*>(smem + L::flag);
     double* sD = reinterpret_cast<double*>(smem + L::D);
     if (tid == 0) {
         mbar_init(bar, 1);
@@ -130,50 +184,18 @@ __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, un
     }
     for (int x = tid; x < L::N2; x += NT) sD[x] = P.D[x];
     __syncthreads();
-    const long long S = P.stride;
     const long long g0 = static_cast<long long>(e0) * L::N3;
     FaceGather<face_points_per_thread<N, KS>()> G;
-    if (tid == 0) {
-        const int nvalid = min(EPB, P.nelt - e0);
-        const long long a0 = g0 & ~1ll, a1 = (g0 + static_cast<long long>(nvalid) * L::N3 + 1) & ~1ll;
-        const unsigned ub = static_cast<unsigned>((a1 - a0) * 8);
-        const long long c0 = static_cast<long long>(e0) * 6, c1 = c0 + 6 * nvalid;
-        const long long ca0 = c0 & ~3ll, ca1 = (c1 + 3) & ~3ll;
-        const unsigned cb = static_cast<unsigned>((ca1 - ca0) * 4);
-        const unsigned gb = static_cast<unsigned>(nvalid * sizeof(ElemGeo));
-        mbar_arrive_expect_tx(bar, (KSM ? 12 : 6) * ub + gb + cb);
-        double* su = reinterpret_cast<double*>(smem + L::u0);
-#pragma unroll
-        for (int c = 0; c < 6; ++c) bulk_g2s(su + c * L::CSR, P.u_in + c * S + a0, ub, bar);
-        if constexpr (KSM) {
-            double* sk = reinterpret_cast<double*>(smem + L::k0);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) bulk_g2s(sk + c * L::CSR, P.k + c * S + a0, ub, bar);
-        } else {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) bulk_prefetch_l2(P.k + c * S + a0, ub);
-        }
-        bulk_g2s(smem + L::geo0, P.geo + e0, gb, bar);
-        bulk_g2s(smem + L::conn0, P.conn + ca0, cb, bar);
-    }
+    if (tid == 0) bulk_issue<N, EPB, KSM>(P, e0, smem);
     if constexpr (EARLY) gather2<N, GEO, KS, EPB, false, false>(P, e0, nullptr, nullptr, tid, G);
-    if (tid == 0) *flag = mbar_wait(bar, 0) ? 1 : 0;
-    __syncthreads();
-    if (!*flag) {
-        if (tid == 0) {
-            report(P, kErrTileWait);
-            mbar_wait(bar, 0);  // bounded: the copies must not land in a finished block
-        }
-        return;
-    }
-    mbar_test(bar, 0);  // the phase is complete: acquire the tile for this thread
+    if (!bulk_wait_tile<N, EPB, KSM>(P, smem, tid)) return;
     const int off = static_cast<int>(g0 & 1);
     const double* su = reinterpret_cast<const double*>(smem + L::u0) + off;
     const double* sk = KSM ? reinterpret_cast<const double*>(smem + L::k0) + off : nullptr;
     const ElemGeo* sg = reinterpret_cast<const ElemGeo*>(smem + L::geo0);
     const int* sc = reinterpret_cast<const int*>(smem + L::conn0) + ((e0 * 6) & 3);
     double* sflux = reinterpret_cast<double*>(smem + L::flux0);
-    compute2<N, GEO, false, KS, EPB, true, false, CONSTD, EARLY, false, DSMEM, CtaBar, L::CSR, KSM>(
+    compute2<N, GEO, false, KS, EPB, true, false, CONSTD, EARLY, false, DSMEM, CtaBar, L::CSR, KSM, VROW>(
         P, e0, su, sg, sc, sD, sflux, nullptr, tid, G, Dc, CtaBar(), sk);
 }
 
@@ -197,20 +219,20 @@ __device__ __forceinline__ int bulk_tile_index(const StageParams& P, int b) {
 }
 
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL>
+          bool ZCOL, bool VROW>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage_bulk_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int t = bulk_tile_index<EPB, ZCOL>(P, blockIdx.x);
-    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY>(P, t * EPB, smem, threadIdx.x, P.Dc);
+    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW>(P, t * EPB, smem, threadIdx.x, P.Dc);
 }
 
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL>
+          bool ZCOL, bool VROW>
 cudaError_t launch_bulk(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int threads = EPB * KS * N * N;
-    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL>;
+    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL, VROW>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, L::total, KSM ? 1 : 0, MINB};
     static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
     if (cudaError_t e = set_smem_once(kern, L::total, attr_set); e != cudaSuccess) return e;

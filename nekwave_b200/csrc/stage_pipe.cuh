@@ -44,6 +44,8 @@
 #pragma once
 #include "stage_kernel.cuh"
 
+#include <cstdint>
+
 namespace nwb {
 namespace stage {
 
@@ -464,9 +466,42 @@ struct CtaBar {
     __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
+// The N values of a node row p[0..N-1] in shared memory with 16-byte loads.  Even N:
+// p must be 16-byte aligned.  Odd N: the loads start at the 16-byte boundary at or
+// below p, so they also read one neighbouring value (p[-1] or p[N]), which must lie
+// inside the tile's shared memory and is discarded.
+template <int N>
+__device__ __forceinline__ void row_pairs(const double* p, double (&r)[N]) {
+    if constexpr (N % 2 == 0) {
+        const double2* b = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int q = 0; q < N / 2; ++q) {
+            const double2 v = b[q];
+            r[2 * q] = v.x;
+            r[2 * q + 1] = v.y;
+        }
+    } else {
+        const int a = static_cast<int>((reinterpret_cast<uintptr_t>(p) >> 3) & 1);
+        const double2* b = reinterpret_cast<const double2*>(p - a);
+        double w[N + 1];
+#pragma unroll
+        for (int q = 0; q < (N + 1) / 2; ++q) {
+            const double2 v = b[q];
+            w[2 * q] = v.x;
+            w[2 * q + 1] = v.y;
+        }
+#pragma unroll
+        for (int l = 0; l < N; ++l) r[l] = a ? w[l + 1] : w[l];
+    }
+}
+
+// VROW (FP64 field split on unpadded tiles whose components and elements start on
+// 16-byte boundaries for even N: the bulk-copy tile): the r-derivative's node rows
+// are read with 16-byte loads (row_pairs), half the shared loads of that sum.  The
+// arithmetic and its order are unchanged.
 template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
           bool EARLY = false, bool FACEDONE = false, bool DSMEM = false, class Bar = CtaBar,
-          int CSX = 0, bool KSM = false>
+          int CSX = 0, bool KSM = false, bool VROW = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
@@ -486,6 +521,7 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
     static_assert(!KSM || (!PAD && !F32), "k in shared memory: unpadded FP64 tiles");
     static_assert(!SPLIT || KS == 1 || KS == 2, "the field split: one or two threads per column");
     static_assert(!CONSTD || (SPLIT && !F32), "constant-bank D: FP64 field split only");
+    static_assert(!VROW || (SPLIT && !F32 && !PAD && CSX % 2 == 0), "row pairs: FP64 split, unpadded");
 
     const int team = tid / TPE;
     const int lt = tid - team * TPE;
@@ -701,14 +737,23 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
             double rhs[3];
             if constexpr (GEO == GEO_BOX) {
                 TX Vz_r = 0, Vy_r = 0, Vz_s = 0, Vx_s = 0, Vy_t = 0, Vx_t = 0;
+                TX rowz[N], rowy[N];
+                if constexpr (VROW) {
+                    row_pairs<N>(V + 2 * CS + PP * k + RP * j, rowz);
+                    row_pairs<N>(V + 1 * CS + PP * k + RP * j, rowy);
+                }
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TX dr = (DSMEM || !SAME) ? static_cast<TX>(sD[i + l * N]) : static_cast<TX>(Dr[l]);
                     const TX ds = (DSMEM || !SAME) ? static_cast<TX>(sD[j + l * N]) : static_cast<TX>(Ds[l]);
                     const TX dt = CONSTD ? static_cast<TX>(Dc[k + l * N]) : static_cast<TX>(sD[k + l * N]);
-                    const int ir = PP * k + RP * j + l;
                     const int is = PP * k + RP * l + i;
-                    Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
+                    if constexpr (VROW) {
+                        Vz_r += dr * rowz[l]; Vy_r += dr * rowy[l];
+                    } else {
+                        const int ir = PP * k + RP * j + l;
+                        Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
+                    }
                     Vz_s += ds * V[2 * CS + is]; Vx_s += ds * V[0 * CS + is];
                     Vy_t += dt * col[1][l]; Vx_t += dt * col[0][l];
                 }

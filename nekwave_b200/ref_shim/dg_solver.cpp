@@ -30,12 +30,16 @@
 
 #include <cuda_runtime.h>
 
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <exception>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -218,6 +222,134 @@ void device_diagnostics(const DgSolver& solver, double* max_e, double* max_h, do
     nwb_solver* s = reg_get(solver, "device_diagnostics");
     nwb_or_abort(nwb_max_norms(s, max_e, max_h), "device_diagnostics (max norms)");
     nwb_or_abort(nwb_energy(s, energy), "device_diagnostics (energy)");
+}
+
+// ---- SnapshotWriter -------------------------------------------------------------
+// The thread that calls save() owns the solver side: it starts a snapshot into a free
+// pinned buffer (nwb_snapshot_begin: device copy in stream order, host copy on a side
+// stream) and, at the next save() or at finish(), waits for that copy and queues the
+// job.  The worker thread only runs jobs on completed buffers.
+struct SnapshotWriter::State {
+    struct Item {
+        int step;
+        double time;
+        Job job;
+        int buf;
+    };
+    nwb_solver* s = nullptr;
+    size_t n = 0;
+    double* buf[2] = {nullptr, nullptr};
+    int next = 0;
+    // the snapshot in flight (the saving thread only)
+    bool pending = false;
+    Item pend{0, 0.0, Job(), 0};
+    // shared with the worker, under mu
+    std::mutex mu;
+    std::condition_variable cv;
+    bool in_use[2] = {false, false};  // from the snapshot's start to its job's end
+    std::deque<Item> queue;
+    bool busy = false, stop = false;
+    std::exception_ptr err;
+    std::thread worker;
+
+    void run() {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv.wait(lk, [&] { return stop || !queue.empty(); });
+            if (queue.empty()) return;
+            Item it = std::move(queue.front());
+            queue.pop_front();
+            busy = true;
+            const bool skip = err != nullptr;  // after a failed job, drop the rest
+            lk.unlock();
+            std::exception_ptr e;
+            if (!skip) {
+                try {
+                    it.job(it.step, it.time, buf[it.buf]);
+                } catch (...) {
+                    e = std::current_exception();
+                }
+            }
+            lk.lock();
+            if (e && !err) err = e;
+            in_use[it.buf] = false;
+            busy = false;
+            cv.notify_all();
+        }
+    }
+    void hand_over() {
+        nwb_or_abort(nwb_snapshot_wait(s), "SnapshotWriter (snapshot copy)");
+        std::lock_guard<std::mutex> lk(mu);
+        queue.push_back(std::move(pend));
+        pending = false;
+        cv.notify_all();
+    }
+};
+
+SnapshotWriter::SnapshotWriter() : st_(new State()) {}
+
+void SnapshotWriter::save(const DgSolver& solver, int step, double time, Job job) {
+    State& S = *st_;
+    nwb_solver* s = reg_get(solver, "SnapshotWriter::save");
+    if (!S.s) {
+        nwb_solver_info info;
+        nwb_or_abort(nwb_solver_get_info(s, &info), "SnapshotWriter (solver info)");
+        S.n = 6 * static_cast<size_t>(info.npts);
+        for (double*& b : S.buf) {
+            if (cudaHostAlloc(reinterpret_cast<void**>(&b), S.n * sizeof(double), cudaHostAllocDefault) !=
+                cudaSuccess) {
+                std::fprintf(stderr, "[NekWave nwb ERROR] SnapshotWriter: pinned host allocation failed\n");
+                std::abort();
+            }
+        }
+        S.s = s;
+        S.worker = std::thread([&S] { S.run(); });
+    } else if (s != S.s) {
+        std::fprintf(stderr, "[NekWave nwb ERROR] SnapshotWriter: one solver per writer\n");
+        std::abort();
+    }
+    if (S.pending) S.hand_over();
+    const int b = S.next;
+    {
+        std::unique_lock<std::mutex> lk(S.mu);
+        S.cv.wait(lk, [&] { return !S.in_use[b]; });
+        S.in_use[b] = true;
+    }
+    nwb_or_abort(nwb_snapshot_begin(s, S.buf[b], S.n), "SnapshotWriter (snapshot)");
+    S.pending = true;
+    S.pend = State::Item{step, time, std::move(job), b};
+    S.next = b ^ 1;
+}
+
+void SnapshotWriter::finish() {
+    State& S = *st_;
+    if (S.pending) S.hand_over();
+    std::unique_lock<std::mutex> lk(S.mu);
+    S.cv.wait(lk, [&] { return S.queue.empty() && !S.busy; });
+    if (S.err) {
+        std::exception_ptr e = S.err;
+        S.err = nullptr;
+        std::rethrow_exception(e);
+    }
+}
+
+SnapshotWriter::~SnapshotWriter() {
+    State& S = *st_;
+    try {
+        finish();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[NekWave nwb ERROR] SnapshotWriter: a snapshot job failed: %s\n", e.what());
+    } catch (...) {
+        std::fprintf(stderr, "[NekWave nwb ERROR] SnapshotWriter: a snapshot job failed\n");
+    }
+    {
+        std::lock_guard<std::mutex> lk(S.mu);
+        S.stop = true;
+        S.cv.notify_all();
+    }
+    if (S.worker.joinable()) S.worker.join();
+    for (double* b : S.buf)
+        if (b) cudaFreeHost(b);
 }
 
 }  // namespace nwb_dropin

@@ -8,8 +8,14 @@ directory only) whose time loop no longer downloads the full state every step:
   * the per-step DgSolver::downloadState (src/case.cpp:588) becomes a download of
     the probe elements only (nwb_dropin::download_probe_elements), which is all
     ProbeManager::record reads;
-  * a full download is made where the state is written out (the HDF5/VTU save
-    block, src/case.cpp:604-625) and, as before, after the loop;
+  * the save block (src/case.cpp:604-625) runs in the background: its body
+    becomes a job of an nwb_dropin::SnapshotWriter, which copies the state to
+    pinned host memory behind the steps queued so far and runs the job (derived
+    fields, Hdf5Writer::writeStep) on its own thread with that copy, in step
+    order, while the loop goes on; the writer finishes before simulate() returns.
+    Inside the job the names the body uses, state_, currentTime_ and step, refer
+    to the snapshot and its step and time;
+  * the full state is downloaded after the loop, as before;
   * max|E|, max|H| and the energy of the output steps (src/case.cpp:632-634) are
     reduced on the device (nwb_dropin::device_diagnostics).
 
@@ -37,9 +43,18 @@ def transform(src: str) -> str:
                        "nwb_dropin::download_probe_elements(*dgSolver_, probes_, "
                        "mesh_->getNumPointsPerElement(), state_);",
                        after='nvtxRangePushA("Case::downloadState");')
-    out = replace_once(out, "if (hdf5Writer_ && (step % saveFreq == 0 || isFinal)) {",
+    out = replace_once(out, "const int saveFreq = std::max(1, config_.saveFreq);\n",
+                       "const int saveFreq = std::max(1, config_.saveFreq);\n"
+                       "    nwb_dropin::SnapshotWriter snapWriter;  // the save block's background writer\n")
+    out = replace_once(out, "if (hdf5Writer_ && (step % saveFreq == 0 || isFinal)) {\n",
                        "if (hdf5Writer_ && (step % saveFreq == 0 || isFinal)) {\n"
-                       "            dgSolver_->downloadState(state_.data(), state_.size());")
+                       "            snapWriter.save(*dgSolver_, step, currentTime_,\n"
+                       "                            [this, npts](int step, double currentTime_, const double* snap) {\n"
+                       "            const struct { const double* p; const double* data() const { return p; } } "
+                       "state_{snap};\n")
+    end = ("hdf5Writer_->writeStep(step, currentTime_, state_.data(), npts, &derived);\n"
+           "#ifndef USE_HIP\n            nvtxRangePop();\n#endif\n")
+    out = replace_once(out, end, end + "            });\n")
     out = replace_once(out, "double maxE = getMaxE();", "double maxE = 0.0, maxH = 0.0, energy = 0.0;\n"
                        "            nwb_dropin::device_diagnostics(*dgSolver_, &maxE, &maxH, &energy);")
     out = replace_once(out, "double maxH = getMaxH();", "")

@@ -16,6 +16,11 @@ Admission policy:
           ``saturation_nodes`` nodes -- enough to keep HBM busy, so admitting more
           would only stretch every running request.  A request larger than that
           runs on its own, as in the serial path; small ones batch together.
+  "hrrn"  as "sjf", but the waiting requests go in order of highest response ratio
+          (waiting time + service time) / service time, the service time taken
+          proportional to the request's work: short requests still go first
+          while the queue is fresh, and a long one rises as it waits, so it is not
+          starved by a stream of short ones (the tail latency "sjf" pays).
 
 The serial baseline serves the same stream one request at a time with the
 single-mesh FP64 solver (DgSolver), the reference's execution model.
@@ -47,12 +52,20 @@ class Result:
         return self.finished - self.arrival
 
 
+def hrrn_key(req: Cavity, t: float, time_scale: float = 1.0) -> float:
+    """Sort key of the "hrrn" policy at time t: the response ratio (wait + service) /
+    service, highest first, with the service time proportional to the request's
+    DOF-stages (only the order matters, so 1 + wait / work, negated)."""
+    wait = max(0.0, t - req.arrival * time_scale)
+    return -(wait / max(req.dof_stages, 1.0))
+
+
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 512, precision: str = "fp32",
                  chunk: int = 4, energy_every: int = 10, policy: str = "sjf",
                  saturation_nodes: int = 8 << 20):
-        if policy not in ("fifo", "sjf"):
-            raise ValueError("policy must be 'fifo' or 'sjf'")
+        if policy not in ("fifo", "sjf", "hrrn"):
+            raise ValueError("policy must be 'fifo', 'sjf' or 'hrrn'")
         self.pool = CavityPool(hbm_budget_bytes, max_slots=max_slots, precision=precision)
         self.chunk = int(chunk)
         self.energy_every = int(energy_every)
@@ -96,10 +109,12 @@ class Server:
                 nxt += 1
             if self.policy == "sjf":
                 pending.sort(key=lambda i: requests[i].dof_stages)
+            elif self.policy == "hrrn":
+                pending.sort(key=lambda i: hrrn_key(requests[i], t, time_scale))
             resident = sum(requests[i].npts for i, _ in running.values())
             while pending:
                 i = pending[0]
-                if (self.policy == "sjf" and running and
+                if (self.policy != "fifo" and running and
                         resident + requests[i].npts > self.saturation_nodes):
                     break
                 try:

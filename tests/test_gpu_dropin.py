@@ -67,7 +67,9 @@ def test_reference_cli_end_to_end_against_dropin(gpu, tmp_path):
                      "ymax": 1.0, "zmin": 0.0, "zmax": 1.0, "periodic": "all"},
             "numerics": {"order": 8, "cfl": 0.5, "flux_type": "central"},
             "time": {"num_steps": 50},
-            "output": {"output_frequency": 10, "export_fields": False, "export_format": "csv"}}
+            # snapshots every 25 steps: the devdiag Case writes them in the background
+            "output": {"output_frequency": 10, "export_fields": True, "export_format": "hdf5",
+                       "save_frequency": 25}}
     out = {}
     for name, exe in (("reference", REF_CLI), ("dropin", os.path.join(DROPIN, "nekwave"))):
         d = tmp_path / name
@@ -103,7 +105,7 @@ def test_device_diagnostics_front_end_on_a_nonzero_wave(gpu, tmp_path):
     the drop-in on libnwb with the reference's per-step full download and host
     diagnostics, and the drop-in with the device-diagnostics Case (probe elements
     only per step, max|E|, max|H| and energy reduced on the device, full state at
-    save steps and at the end).  The energy histories (step, time, max|E|, max|H|,
+    save steps through the background SnapshotWriter, and at the end).  The energy histories (step, time, max|E|, max|H|,
     energy) and probe histories agree to the 9 significant digits the front end
     prints; the simulate() wall times are recorded (cli_devdiag.json)."""
     from nekwave_b200.workloads import single_mesh
@@ -114,7 +116,9 @@ def test_device_diagnostics_front_end_on_a_nonzero_wave(gpu, tmp_path):
             "numerics": {"order": 8, "cfl": 0.5, "flux_type": "central"},
             "time": {"num_steps": 100},
             "probes": [[0.31, 0.52, 0.47], [0.5, 0.5, 0.5], [0.77, 0.13, 0.9], [0.05, 0.95, 0.6]],
-            "output": {"output_frequency": 10, "export_fields": False, "export_format": "csv"}}
+            # snapshots every 25 steps: the devdiag Case writes them in the background
+            "output": {"output_frequency": 10, "export_fields": True, "export_format": "hdf5",
+                       "save_frequency": 25}}
     runs = {"reference": PULSE_REF, "dropin": os.path.join(DROPIN, "pulse-case"),
             "devdiag": os.path.join(DROPIN, "pulse-case-devdiag")}
     out = {}
@@ -149,3 +153,19 @@ def test_device_diagnostics_front_end_on_a_nonzero_wave(gpu, tmp_path):
         "case": "periodic 32^3, 8 points, central, seeded Gaussian Ez, 100 steps, 4 probes, "
                 "diagnostics every 10 steps, Case::simulate",
         **{f"{k}_simulate_s": v["simulate_s"] for k, v in out.items()}})
+
+
+SNAPSHOT_CHECK = os.path.join(DROPIN, "snapshot-check")
+
+
+@pytest.mark.skipif(not os.path.exists(SNAPSHOT_CHECK), reason="snapshot-check not built")
+@pytest.mark.parametrize("N,nel,steps,every", [(6, 6, 40, 5), (8, 4, 21, 1)])
+def test_snapshot_writer_matches_synchronous_downloads(gpu, N, nel, steps, every):
+    """The devdiag front end's background writer (nwb_dropin::SnapshotWriter): the
+    states its jobs receive, with their steps and times, equal bit for bit the
+    synchronous downloads the reference's Case::simulate makes at the same steps,
+    also when every step is a save and the jobs lag the loop."""
+    r = subprocess.run([SNAPSHOT_CHECK, str(N), str(nel), str(steps), str(every)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert f"saves {steps // every} / {steps // every}" in r.stdout and "equal" in r.stdout

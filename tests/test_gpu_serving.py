@@ -15,7 +15,7 @@ def small_stream(n=8, rate=200.0):
     return serving_requests(n, rate, seed=5, max_nel=5, max_order=5)
 
 
-@pytest.mark.parametrize("policy", ["fifo", "sjf"])
+@pytest.mark.parametrize("policy", ["fifo", "sjf", "hrrn"])
 def test_each_request_same_alone_and_in_the_mix(gpu, policy):
     reqs = small_stream()
     srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=3, energy_every=1, policy=policy,

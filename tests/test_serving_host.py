@@ -108,7 +108,7 @@ def run(policy, reqs, budget=1 << 40, saturation=1 << 40, chunk=4):
     return results
 
 
-@pytest.mark.parametrize("policy", ["fifo", "sjf"])
+@pytest.mark.parametrize("policy", ["fifo", "sjf", "hrrn"])
 def test_every_request_completes_with_its_histories(fake, policy):
     reqs = requests(SIZES)
     results = run(policy, reqs)
@@ -149,3 +149,26 @@ def test_full_pool_defers_admission(fake):
     results = run("fifo", reqs, budget=budget)
     assert all(r is not None for r in results)
     assert fake[0].max_resident * BYTES_PER_NODE <= budget
+
+
+def test_hrrn_orders_by_response_ratio():
+    """A long request that has waited rises above short ones that have not; among
+    requests that waited alike, shorter work goes first (as in sjf)."""
+    big, small, mid = requests([(6, 4, 40), (4, 2, 10), (6, 4, 20)])  # work 110 : 1 : 55
+    big.arrival, small.arrival, mid.arrival = 0.0, 9.99, 9.99
+    order = sorted([small, big, mid], key=lambda r: serving.hrrn_key(r, 10.0))
+    # the long one waited 1000x longer for 110x the work: its ratio is the highest
+    assert order == [big, small, mid]
+    early = sorted([small, big, mid], key=lambda r: serving.hrrn_key(r, 9.99 + 1e-12))
+    assert early[0] is big  # the others have hardly waited
+    fresh = sorted([big, mid, small], key=lambda r: serving.hrrn_key(r, 20.0, time_scale=0.0))
+    assert fresh == [small, mid, big]  # equal waits: shortest work first
+
+
+def test_hrrn_keeps_resident_nodes_under_saturation(fake):
+    reqs = requests(SIZES)
+    sat = 300_000
+    results = run("hrrn", reqs, saturation=sat)
+    assert all(r is not None for r in results)
+    for npts, _, resident, running_before in fake[0].log:
+        assert resident <= sat or running_before == 0
