@@ -84,13 +84,16 @@ def parse():
     p.add_argument("--workload", choices=["c2", "c3", "batch", "serve"], default="c2",
                    help="c2: periodic 32^3 N=8 (default, the headline); batch: 256 uneven PEC "
                         "cavities in one pool; serve: Poisson request stream")
-    p.add_argument("--rates", type=str, default="0.5,1,2",
+    p.add_argument("--rates", type=str, default="0.25,0.5,1,2,4",
                    help="serve: arrival rates as multiples of the measured serial service rate")
-    p.add_argument("--requests", type=int, default=24, help="serve: requests per rate")
+    p.add_argument("--requests", type=int, default=100, help="serve: requests per rate")
     p.add_argument("--policies", type=str, default="fifo,sjf", help="serve: admission policies")
-    p.add_argument("--serial-rates", type=str, default=None,
-                   help="serve: rates (multiples) at which the serial path is run (default: --rates; "
-                        "'none' for none)")
+    p.add_argument("--serial-replay", action="store_true",
+                   help="serve: replay the stream in real time on the serial path at every rate "
+                        "(default: its schedule from service times measured once)")
+    p.add_argument("--t-scale", type=float, default=1.0,
+                   help="serve: final times T ~ U[0.5,2] scaled by this factor (fewer steps per "
+                        "request; same sizes and orders)")
     p.add_argument("--serial-rate-per-s", type=float, default=0.0,
                    help="serve: the serial service rate (solves/s) to scale the arrivals by, "
                         "instead of measuring it (lets a sweep be split over runs)")
@@ -393,27 +396,34 @@ def run_batch(args, rank, world):
 
 def run_serve(args, rank, world):
     """Poisson stream of cavity solves served with continuous batching; p50/p99
-    latency and solves/s per arrival rate, next to the serial FP64 path."""
+    latency and solves/s per arrival rate, next to the serial FP64 path.
+
+    The serial path takes one request at a time in arrival order, so its schedule
+    follows from each request's service time: finish_i = max(arrival_i,
+    finish_{i-1}) + service_i.  The service times are measured once, the requests
+    run back to back on the single-mesh solver (serving.serial_service_times), and
+    the serial latencies at every rate come from that schedule; --serial-replay
+    instead replays the stream in real time at each rate."""
     import torch
-    from nekwave_b200.serving import Server, latency_stats, serve_serial
+    from nekwave_b200.serving import (Server, fifo_finish_times, latency_stats, latency_summary,
+                                      serial_service_times, serve_serial)
     from nekwave_b200.workloads import serving_requests
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     n = args.requests
-    # serial service rate: the serial path's GDOF-stage/s on a few requests over the
-    # mean work of a request of this distribution (2000 samples, no GPU work)
-    mean_work = float(np.mean([c.dof_stages for c in serving_requests(2000, 1.0, seed=args.seed + 7)]))
-    if args.serial_rate_per_s > 0:
-        mu = args.serial_rate_per_s
-        serial_rate = mu * mean_work
-    else:
-        calib = serving_requests(4, 1e9, seed=args.seed + 1000)
-        _, cal_wall = serve_serial(calib, precision="fp64")
-        serial_rate = sum(c.dof_stages for c in calib) / cal_wall
-        mu = serial_rate / mean_work
-    rows = []
+    base = serving_requests(n, 1.0, seed=args.seed + 100, t_scale=args.t_scale)  # arrivals at 1/s
+    work = sum(c.dof_stages for c in base)
     budget = int(float(os.environ.get("NWB_SERVE_BUDGET_GB", "100")) * (1 << 30))
-    base = serving_requests(n, 1.0, seed=args.seed + 100)  # one request set, arrivals at rate 1/s
-    for mult in [float(x) for x in args.rates.split(",")]:
+    if args.serial_rate_per_s > 0:
+        svc = None
+        mu = args.serial_rate_per_s
+    else:
+        solve_warm = serving_requests(2, 1.0, seed=args.seed + 1000, t_scale=0.05)
+        serial_service_times(solve_warm)                     # first-use set-up off the clock
+        svc = serial_service_times(base)
+        mu = n / float(svc.sum())                            # serial solves/s on this request set
+    rates = [float(x) for x in args.rates.split(",")]
+    rows = []
+    for mult in rates:
         reqs = [dataclasses.replace(r, arrival=r.arrival / (mult * mu)) for r in base]
         for policy in [x for x in args.policies.split(",") if x]:
             srv = Server(budget, max_slots=512, precision=args.precision, policy=policy)
@@ -422,16 +432,24 @@ def run_serve(args, rank, world):
             st = latency_stats(res)
             rows.append(dict(policy=policy, rate_multiple=mult, rate_per_s=mult * mu,
                              solves_per_s=n / wall, p50_s=st["p50"], p99_s=st["p99"],
-                             mean_s=st["mean"],
-                             gdof_stage_per_s=sum(r.dof_stages for r in reqs) / wall / 1e9))
+                             mean_s=st["mean"], max_s=st["max"],
+                             gdof_stage_per_s=work / wall / 1e9))
     serial = []
-    srates = args.rates if args.serial_rates is None else args.serial_rates
-    for mult in ([] if srates == "none" else [float(x) for x in srates.split(",")]):
-        serial_reqs = [dataclasses.replace(r, arrival=r.arrival / (mult * mu)) for r in base]
-        sres, swall = serve_serial(serial_reqs, precision="fp64")
-        sst = latency_stats(sres)
+    for mult in rates:
+        arr = np.array([r.arrival / (mult * mu) for r in base])
+        if args.serial_replay or svc is None:
+            serial_reqs = [dataclasses.replace(r, arrival=a) for r, a in zip(base, arr)]
+            sres, swall = serve_serial(serial_reqs, precision="fp64")
+            sst = latency_stats(sres)
+            how = "replayed in real time"
+        else:
+            fin = fifo_finish_times(arr, svc)
+            sst = latency_summary(fin - arr)
+            swall = float(fin.max())
+            how = "schedule from the measured service times"
         serial.append(dict(rate_multiple=mult, rate_per_s=mult * mu, solves_per_s=n / swall,
-                           p50_s=sst["p50"], p99_s=sst["p99"], mean_s=sst["mean"]))
+                           p50_s=sst["p50"], p99_s=sst["p99"], mean_s=sst["mean"],
+                           max_s=sst["max"], gdof_stage_per_s=work / swall / 1e9, how=how))
     best = max(rows, key=lambda r: r["solves_per_s"]) if rows else {"solves_per_s": None}
     return {"metric": "solves/s", "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": world,
             "steps": n, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
@@ -439,9 +457,13 @@ def run_serve(args, rank, world):
             "dtype": "f64" if args.precision == "fp64" else "f32-bulk/f64-lsrk",
             "data": "synthetic Poisson stream (seeded)",
             "config": dict(workload="serving_poisson_pec_cavities", requests_per_rate=n,
-                           serial_service_rate_per_s=mu, serial_gdof_stage_per_s=serial_rate / 1e9,
-                           mean_request_gdof_stage=mean_work / 1e9, max_elements_per_dir=48,
-                           points_per_dir="4..9", budget_gb=budget / (1 << 30)),
+                           final_time_scale=args.t_scale,
+                           serial_service_rate_per_s=mu,
+                           serial_gdof_stage_per_s=(mu * work / n / 1e9),
+                           mean_request_gdof_stage=work / n / 1e9, max_elements_per_dir=48,
+                           points_per_dir="4..9", budget_gb=budget / (1 << 30),
+                           serial_service_s=(dict(p50=float(np.median(svc)), mean=float(svc.mean()),
+                                                  max=float(svc.max())) if svc is not None else None)),
             "serving": rows,
             "serial_fp64": serial,
             "serial_pattern": "one request at a time with the single-mesh FP64 solver, a step at a "
@@ -547,21 +569,28 @@ def main():
         solver.downloadState(hnp)          # D2H of the step's result state
     barrier()
     e2e_block = job_rate(6 * npts * 5 * e2e_steps, max_over_ranks(time.perf_counter() - t0), world)
-    # (2) the same copies through the asynchronous snapshot: step i's result is copied
-    # on the device in stream order and then to the host on a side stream, while step
-    # i+1 uploads and runs (the host link carries both directions at once); the last
-    # snapshot is waited for inside the timed region
+    # (2) the same copies pipelined: each step's input state is uploaded
+    # asynchronously (host -> staging on an upload stream while the previous step
+    # runs, then staging -> state in stream order) and its result leaves through the
+    # asynchronous snapshot (device copy in stream order, then device -> host on a
+    # side stream), so the host link carries step i+1's input and step i's result at
+    # the same time while the GPU steps; the last snapshot is waited for inside the
+    # timed region.  Every step still moves its whole input in and its whole result out.
     host_out = torch.empty(6 * npts, dtype=torch.float64).pin_memory()
     hout = host_out.numpy()
-    solver.snapshotBegin(hout)             # set-up of the snapshot buffer, untimed
+    solver.snapshotBegin(hout)             # set-up of the snapshot and staging buffers, untimed
     solver.snapshotWait()
+    solver.uploadBegin(hnp)
+    solver.uploadWait()
+    solver.sync()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        solver.uploadState(hnp)            # H2D of the step's input state (pinned)
-        solver.step(dt, 0.0)               # one LSRK45 step
+        solver.uploadBegin(hnp)            # H2D of the step's input state (pinned)
+        solver.steps(dt, 1, sync=False)    # one LSRK45 step, queued behind the upload
         solver.snapshotBegin(hout)         # D2H of the step's result state
     solver.snapshotWait()
+    solver.uploadWait()
     barrier()
     e2e_value = job_rate(6 * npts * 5 * e2e_steps, max_over_ranks(time.perf_counter() - t0), world)
     del ctypes, host_out
@@ -616,9 +645,11 @@ def main():
             "e2e": {"value": e2e_value, "unit": METRIC,
                     "h2d_bytes_per_step": 6 * npts * 8, "d2h_bytes_per_step": 6 * npts * 8,
                     "steps": e2e_steps,
-                    "pattern": "uploadState (pinned) + step + snapshotBegin (asynchronous D2H of "
-                               "the result, overlapping the next step's upload) per step; the last "
-                               "snapshot waited for inside the timed region",
+                    "pattern": "uploadBegin (asynchronous H2D of the step's input from pinned "
+                               "memory) + step + snapshotBegin (asynchronous D2H of its result) per "
+                               "step, pipelined so that step i+1's upload and step i's download "
+                               "share the host link while the GPU steps; the last snapshot and "
+                               "upload waited for inside the timed region",
                     "blocking": {"value": e2e_block, "pattern": "uploadState (pinned) + step + "
                                  "downloadState per step, the reference's blocking calls"}},
         }

@@ -195,6 +195,18 @@ nwb_status nwb_probe_read(nwb_solver* s, double* out);
  * the caller only needs the state at save steps. */
 nwb_status nwb_snapshot_begin(nwb_solver* s, double* host, size_t n);
 nwb_status nwb_snapshot_wait(nwb_solver* s);
+/* Asynchronous upload, the reverse of the snapshot: replaces DgSolver::uploadState
+ * (src/dg_solver.cpp:243-262) where the caller streams states in.  The host state
+ * (6*npts doubles, [6][npts]; pinned memory lets the copy overlap) is copied on an
+ * upload stream into a device staging buffer while the steps already queued run,
+ * then, in the solver's stream order, into the current state: steps queued after
+ * this call start from it.  The host buffer must stay unchanged until
+ * nwb_upload_wait returns.  A second begin reuses the staging buffer once the
+ * first upload has been copied out of it (on the device, without a host wait).
+ * With nwb_snapshot_begin this pipelines upload, step and download of successive
+ * states: the host link carries one state in and one out while the GPU steps. */
+nwb_status nwb_upload_begin(nwb_solver* s, const double* host, size_t n);
+nwb_status nwb_upload_wait(nwb_solver* s);
 nwb_status nwb_solver_destroy(nwb_solver* s);
 
 /* Introspection used by tests and the benchmark. */
@@ -243,7 +255,8 @@ nwb_status nwb_energy_noalloc(const double* d_state, long long stride, int N, in
 
 /* Launch shape of the fused stage kernel.  nwb_solver_autotune times every
  * shape for this mesh (reps launches each, with a = b = dt = 0 so the state is
- * left as it was) and keeps the fastest; ms_out (optional, ms_cap entries)
+ * left as it was) and keeps the fastest, or the default shape (variant 0) when
+ * it is within 1% of the fastest (timing noise); ms_out (optional, ms_cap entries)
  * receives the per-shape average launch time.  Neither call has a counterpart
  * in the reference, which has one fixed launch shape per kernel. */
 nwb_status nwb_solver_set_variant(nwb_solver* s, int variant);

@@ -87,6 +87,8 @@ SIGNATURES = {
     "nwb_probe_read": (C.c_int, [C.c_void_p, _D]),
     "nwb_snapshot_begin": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
     "nwb_snapshot_wait": (C.c_int, [C.c_void_p]),
+    "nwb_upload_begin": (C.c_int, [C.c_void_p, _D, C.c_size_t]),
+    "nwb_upload_wait": (C.c_int, [C.c_void_p]),
     "nwb_solver_destroy": (C.c_int, [C.c_void_p]),
     "nwb_solver_get_info": (C.c_int, [C.c_void_p, C.POINTER(SolverInfo)]),
     "nwb_solver_device_state": (C.c_int, [C.c_void_p, C.POINTER(_D), C.POINTER(C.c_void_p)]),

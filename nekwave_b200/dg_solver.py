@@ -173,6 +173,19 @@ class DgSolver:
         check(_lib.lib().nwb_snapshot_wait(self._need()))
         self._snap = None
 
+    def uploadBegin(self, host: np.ndarray) -> None:
+        """Start an asynchronous upload of host (6*npts doubles, C-contiguous; pinned
+        memory lets it overlap the steps already queued): steps queued afterwards
+        start from it.  host must stay unchanged until uploadWait."""
+        if host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
+            raise ValueError("host must be a C-contiguous float64 array")
+        self._up = host  # keep it alive until the copy lands
+        check(_lib.lib().nwb_upload_begin(self._need(), host.ctypes.data_as(_lib._D), host.size))
+
+    def uploadWait(self) -> None:
+        check(_lib.lib().nwb_upload_wait(self._need()))
+        self._up = None
+
     def info(self) -> dict:
         h = self._need()
         i = SolverInfo()

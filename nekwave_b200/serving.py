@@ -62,18 +62,34 @@ def hrrn_key(req: Cavity, t: float, time_scale: float = 1.0) -> float:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 512, precision: str = "fp32",
-                 chunk: int = 4, energy_every: int = 10, policy: str = "sjf",
-                 saturation_nodes: int = 8 << 20):
+                 chunk: int | None = None, energy_every: int = 10, policy: str = "sjf",
+                 saturation_nodes: int = 8 << 20, chunk_ms: float = 3.0):
         if policy not in ("fifo", "sjf", "hrrn"):
             raise ValueError("policy must be 'fifo', 'sjf' or 'hrrn'")
         self.pool = CavityPool(hbm_budget_bytes, max_slots=max_slots, precision=precision)
-        self.chunk = int(chunk)
+        self.chunk = None if chunk is None else int(chunk)
+        self.chunk_ms = float(chunk_ms)
         self.energy_every = int(energy_every)
         self.policy = policy
         self.saturation_nodes = int(saturation_nodes)
 
     def close(self):
         self.pool.close()
+
+    # HBM bytes one step moves per resident node (32 B per DOF-stage, 6 DOF, 5 stages)
+    # and a conservative rate for them: the estimate only sizes the chunks
+    STEP_BYTES_PER_NODE = 32 * 6 * 5
+    EST_BYTES_PER_S = 3.5e12
+    MIN_STEP_S = 25e-6   # five launches of a nearly empty step graph
+
+    def chunk_steps(self, resident_nodes: int) -> int:
+        """Steps queued per round: a fixed chunk when one was given, else enough
+        steps for about chunk_ms of GPU work at the resident size (4..64), so that a
+        round's host bookkeeping stays well below the GPU time it runs behind."""
+        if self.chunk is not None:
+            return self.chunk
+        step_s = max(self.MIN_STEP_S, resident_nodes * self.STEP_BYTES_PER_NODE / self.EST_BYTES_PER_S)
+        return int(min(64, max(4, round(self.chunk_ms * 1e-3 / step_s))))
 
     def admit(self, req: Cavity):
         s = self.pool.add_box(req.N, req.nel, req.lo, req.hi, req.c0, req.dt, req.nsteps,
@@ -131,7 +147,7 @@ class Server:
                         time.sleep(min(wait, 0.05))
                 continue
             if running:
-                self.pool.step(self.chunk)
+                self.pool.step(self.chunk_steps(resident))
             if snapshot:
                 status, _ = self.pool.query_end()
                 # result copies queued before that snapshot have landed
@@ -159,8 +175,6 @@ def serve_serial(requests, precision="fp64", time_scale: float = 1.0, energy_eve
     state; the probes (ProbeManager::record) and the energy are evaluated on the
     device and only their values are read back, which spares it the reference's
     full per-step download."""
-    from . import DgSolver
-    from .pool import box_probes
     order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
     results = [None] * len(requests)
     t0 = time.perf_counter()
@@ -170,31 +184,73 @@ def serve_serial(requests, precision="fp64", time_scale: float = 1.0, energy_eve
         if wait > 0:
             time.sleep(wait)
         ta = time.perf_counter() - t0
-        s = DgSolver(precision)
-        s.initializeBox(req.N, req.nel, req.lo, req.hi, req.c0, periodic=req.periodic)
-        s.initPulse(req.pulses)
-        np_ = len(req.probes)
-        if np_:
-            off, w = box_probes(req.N, req.nel, req.lo, req.hi, req.probes)
-            s.probeSetup(off, w)
-        probes = np.zeros((req.nsteps + 1, np_, 6))
-        energy = np.full(req.nsteps + 1, np.nan)
-        energy[0] = s.energy()
-        if np_:
-            probes[0] = s.probeRead()
-        for n in range(1, req.nsteps + 1):
-            s.step(req.dt, 0.0)
-            if np_:
-                probes[n] = s.probeRead()
-            if n % energy_every == 0 or n == req.nsteps:
-                energy[n] = s.energy()
-        s.finalize()
+        probes, energy = solve_one(req, precision, energy_every)
         tf = time.perf_counter() - t0
         results[i] = Result(i, req.arrival * time_scale, ta, tf, probes, energy, retired=tf)
     return results, time.perf_counter() - t0
 
 
+def solve_one(req: Cavity, precision: str = "fp64", energy_every: int = 10):
+    """One request alone on the single-mesh solver, as serve_serial runs it: a
+    step at a time, the 8 probes read after every step, the energy every
+    energy_every steps and at the end.  Returns (probes, energy)."""
+    from . import DgSolver
+    from .pool import box_probes
+    s = DgSolver(precision)
+    s.initializeBox(req.N, req.nel, req.lo, req.hi, req.c0, periodic=req.periodic)
+    s.initPulse(req.pulses)
+    np_ = len(req.probes)
+    if np_:
+        off, w = box_probes(req.N, req.nel, req.lo, req.hi, req.probes)
+        s.probeSetup(off, w)
+    probes = np.zeros((req.nsteps + 1, np_, 6))
+    energy = np.full(req.nsteps + 1, np.nan)
+    energy[0] = s.energy()
+    if np_:
+        probes[0] = s.probeRead()
+    for n in range(1, req.nsteps + 1):
+        s.step(req.dt, 0.0)
+        if np_:
+            probes[n] = s.probeRead()
+        if n % energy_every == 0 or n == req.nsteps:
+            energy[n] = s.energy()
+    s.finalize()
+    return probes, energy
+
+
+def serial_service_times(requests, precision: str = "fp64", energy_every: int = 10):
+    """Service time of every request on the serial path (solve_one), the requests
+    run back to back in list order with nothing else on the GPU."""
+    out = []
+    for req in requests:
+        t = time.perf_counter()
+        solve_one(req, precision, energy_every)
+        out.append(time.perf_counter() - t)
+    return np.asarray(out)
+
+
+def fifo_finish_times(arrivals, service):
+    """Finish times of a server that takes one request at a time in arrival order
+    (the serial path): finish_i = max(arrival_i, finish_{i-1}) + service_i.  Given
+    each request's service time this is the serial server's schedule exactly, for
+    any arrival times, since its service does not depend on the queue."""
+    arrivals = np.asarray(arrivals, float)
+    service = np.asarray(service, float)
+    order = np.argsort(arrivals, kind="stable")
+    fin = np.empty_like(arrivals)
+    t = 0.0
+    for i in order:
+        t = max(t, arrivals[i]) + service[i]
+        fin[i] = t
+    return fin
+
+
 def latency_stats(results):
     lat = np.array([r.latency for r in results if r is not None])
+    return latency_summary(lat)
+
+
+def latency_summary(lat):
+    lat = np.asarray(lat, float)
     return dict(n=int(lat.size), p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
                 mean=float(lat.mean()), max=float(lat.max()))

@@ -147,11 +147,14 @@ def batch_instances(n=256, seed=0, steps=400):
     return out
 
 
-def serving_requests(n, rate, seed=0, max_nel=48, max_order=8):
+def serving_requests(n, rate, seed=0, max_nel=48, max_order=8, t_scale=1.0):
     """Poisson stream (rate requests/s) of PEC cavity solves sized as the batch
     instances but with up to max_nel elements per direction and order <= 8;
     each runs to a final time T ~ U[0.5,2] (dt = T / ceil(T / dt_cfl), so the last
-    step lands on T) and returns 8 probe traces and its energy history."""
+    step lands on T) and returns 8 probe traces and its energy history.
+    t_scale < 1 shortens every final time by that factor (same sizes, orders,
+    pulses and probes; fewer steps), for latency sweeps that must fit a time
+    budget."""
     r = rng(seed)
     t = 0.0
     out = []
@@ -162,7 +165,7 @@ def serving_requests(n, rate, seed=0, max_nel=48, max_order=8):
         N = int(r.integers(3, max_order + 1)) + 1
         lo, hi = (0.0, 0.0, 0.0), tuple(float(e) for e in edges)
         sig = float(r.uniform(0.05, 0.15) * edges.min())
-        T = float(r.uniform(0.5, 2.0))
+        T = float(r.uniform(0.5, 2.0)) * t_scale
         dt_cfl = CFL * box_dxmin(N, nel, lo, hi)
         nsteps = max(1, math.ceil(T / dt_cfl))
         probes = [tuple(float(v) for v in np.asarray(lo) + (np.asarray(hi) - np.asarray(lo)) *

@@ -172,3 +172,48 @@ def test_hrrn_keeps_resident_nodes_under_saturation(fake):
     assert all(r is not None for r in results)
     for npts, _, resident, running_before in fake[0].log:
         assert resident <= sat or running_before == 0
+
+
+def test_fifo_finish_times_match_a_one_at_a_time_simulation():
+    """The serial path's schedule from service times equals a step-by-step simulation
+    of a server that takes one request at a time in arrival order."""
+    r = np.random.Generator(np.random.PCG64(5))
+    for rate in (0.25, 1.0, 4.0):
+        arr = np.cumsum(r.exponential(1.0 / rate, 200))
+        svc = r.exponential(1.0, 200)
+        perm = r.permutation(200)             # requests need not be listed in arrival order
+        fin = serving.fifo_finish_times(arr[perm], svc[perm])
+        clock, want = 0.0, np.empty(200)
+        for i in range(200):                  # arr is sorted: serve in index order
+            start = arr[i] if arr[i] > clock else clock
+            clock = start + svc[i]
+            want[i] = clock
+        assert np.array_equal(fin, want[perm])
+        lat = fin - arr[perm]
+        assert (lat >= svc[perm] - 1e-12).all()
+    st = serving.latency_summary([1.0, 2.0, 3.0])
+    assert st["p50"] == 2.0 and st["max"] == 3.0 and st["n"] == 3
+
+
+def test_serving_requests_final_time_scale():
+    """t_scale shortens the final times only: sizes, orders, pulses, probes and
+    arrivals are those of the unscaled stream."""
+    from nekwave_b200.workloads import serving_requests
+    a = serving_requests(20, 1.0, seed=3)
+    b = serving_requests(20, 1.0, seed=3, t_scale=0.125)
+    for x, y in zip(a, b):
+        assert (x.N, x.nel, x.lo, x.hi, x.arrival) == (y.N, y.nel, y.lo, y.hi, y.arrival)
+        assert x.pulses == y.pulses and x.probes == y.probes
+        assert abs(y.T - 0.125 * x.T) < 1e-15 * x.T
+        assert y.nsteps <= x.nsteps and abs(y.dt * y.nsteps - y.T) < 1e-12
+
+
+def test_adaptive_chunk_follows_the_resident_size(monkeypatch):
+    """Without a fixed chunk the server queues about chunk_ms of GPU work per round:
+    many steps while few nodes are resident, four once a step alone takes longer."""
+    monkeypatch.setattr(serving, "CavityPool", FakePool)
+    srv = serving.Server(1 << 40, max_slots=16, precision="fp64", policy="fifo")
+    small, mid, big = srv.chunk_steps(1000), srv.chunk_steps(1 << 20), srv.chunk_steps(64 << 20)
+    assert small == 64 and big == 4 and 4 <= mid <= 64 and small >= mid >= big
+    fixed = serving.Server(1 << 40, max_slots=16, precision="fp64", chunk=7)
+    assert fixed.chunk_steps(1000) == 7 and fixed.chunk_steps(64 << 20) == 7
