@@ -582,7 +582,7 @@ def main():
     solver.snapshotWait()
     solver.uploadBegin(hnp)
     solver.uploadWait()
-    solver.sync()
+    torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):

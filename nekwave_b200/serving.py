@@ -21,6 +21,14 @@ Admission policy:
           proportional to the request's work: short requests still go first
           while the queue is fresh, and a long one rises as it waits, so it is not
           starved by a stream of short ones (the tail latency "sjf" pays).
+  "guard" as "hrrn", but a request that has waited longer than a guard goes first,
+          oldest first, and the requests behind it wait until it fits under the
+          node limit: a bound on how long a large request can be passed over, so
+          that under overload the tail latency is no worse than first come, first
+          served, while the short requests still batch ahead.  The guard is
+          ``guard_s`` seconds, or by default ``guard_services`` times the mean
+          estimated service time of the requests seen so far (their work at a
+          rate of EST_BYTES_PER_S of HBM traffic), which scales with the stream.
 
 The serial baseline serves the same stream one request at a time with the
 single-mesh FP64 solver (DgSolver), the reference's execution model.
@@ -63,15 +71,18 @@ def hrrn_key(req: Cavity, t: float, time_scale: float = 1.0) -> float:
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 512, precision: str = "fp32",
                  chunk: int | None = None, energy_every: int = 10, policy: str = "sjf",
-                 saturation_nodes: int = 8 << 20, chunk_ms: float = 3.0):
-        if policy not in ("fifo", "sjf", "hrrn"):
-            raise ValueError("policy must be 'fifo', 'sjf' or 'hrrn'")
+                 saturation_nodes: int = 8 << 20, chunk_ms: float = 3.0,
+                 guard_s: float | None = None, guard_services: float = 16.0):
+        if policy not in ("fifo", "sjf", "hrrn", "guard"):
+            raise ValueError("policy must be 'fifo', 'sjf', 'hrrn' or 'guard'")
         self.pool = CavityPool(hbm_budget_bytes, max_slots=max_slots, precision=precision)
         self.chunk = None if chunk is None else int(chunk)
         self.chunk_ms = float(chunk_ms)
         self.energy_every = int(energy_every)
         self.policy = policy
         self.saturation_nodes = int(saturation_nodes)
+        self.guard_s = guard_s
+        self.guard_services = float(guard_services)
 
     def close(self):
         self.pool.close()
@@ -90,6 +101,27 @@ class Server:
             return self.chunk
         step_s = max(self.MIN_STEP_S, resident_nodes * self.STEP_BYTES_PER_NODE / self.EST_BYTES_PER_S)
         return int(min(64, max(4, round(self.chunk_ms * 1e-3 / step_s))))
+
+    @classmethod
+    def est_service_s(cls, req: Cavity) -> float:
+        """Service time of a request estimated from its work alone."""
+        return req.npts * req.nsteps * cls.STEP_BYTES_PER_NODE / cls.EST_BYTES_PER_S
+
+    def order_pending(self, pending, requests, t, time_scale=1.0, mean_service_s=0.0):
+        """The waiting requests (indices into requests) in admission order at time t."""
+        if self.policy == "sjf":
+            return sorted(pending, key=lambda i: requests[i].dof_stages)
+        if self.policy in ("hrrn", "guard"):
+            out = sorted(pending, key=lambda i: hrrn_key(requests[i], t, time_scale))
+            if self.policy == "guard":
+                g = self.guard_s if self.guard_s is not None else self.guard_services * mean_service_s
+                waited = lambda i: t - requests[i].arrival * time_scale
+                old = sorted((i for i in out if waited(i) > g), key=lambda i: requests[i].arrival)
+                if old:
+                    olds = set(old)
+                    out = old + [i for i in out if i not in olds]
+            return out
+        return list(pending)  # fifo: arrival order
 
     def admit(self, req: Cavity):
         s = self.pool.add_box(req.N, req.nel, req.lo, req.hi, req.c0, req.dt, req.nsteps,
@@ -116,17 +148,19 @@ class Server:
         fetching = {}           # request index -> (admit time, result buffers in flight)
         snapshot = False        # a status snapshot is queued
         results = [None] * len(requests)
+        seen_s, seen_n = 0.0, 0  # estimated service of the requests arrived so far
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         while nxt < len(arrivals) or pending or running or fetching:
             t = now()
             while nxt < len(arrivals) and requests[arrivals[nxt]].arrival * time_scale <= t:
                 pending.append(arrivals[nxt])
+                seen_s += self.est_service_s(requests[arrivals[nxt]])
+                seen_n += 1
                 nxt += 1
-            if self.policy == "sjf":
-                pending.sort(key=lambda i: requests[i].dof_stages)
-            elif self.policy == "hrrn":
-                pending.sort(key=lambda i: hrrn_key(requests[i], t, time_scale))
+            if pending:
+                pending = self.order_pending(pending, requests, t, time_scale,
+                                             seen_s / max(seen_n, 1))
             resident = sum(requests[i].npts for i, _ in running.values())
             while pending:
                 i = pending[0]

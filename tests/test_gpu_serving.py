@@ -15,11 +15,12 @@ def small_stream(n=8, rate=200.0):
     return serving_requests(n, rate, seed=5, max_nel=5, max_order=5)
 
 
-@pytest.mark.parametrize("policy", ["fifo", "sjf", "hrrn"])
-def test_each_request_same_alone_and_in_the_mix(gpu, policy):
+@pytest.mark.parametrize("policy,chunk", [("fifo", 3), ("sjf", 3), ("hrrn", 3), ("guard", 3),
+                                          ("guard", None)])
+def test_each_request_same_alone_and_in_the_mix(gpu, policy, chunk):
     reqs = small_stream()
-    srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=3, energy_every=1, policy=policy,
-                 saturation_nodes=20000)
+    srv = Server(4 << 30, max_slots=64, precision="fp64", chunk=chunk, energy_every=1, policy=policy,
+                 saturation_nodes=20000, guard_s=0.01)
     mixed, wall = srv.run(reqs)
     srv.close()
     assert all(r is not None for r in mixed)

@@ -217,3 +217,42 @@ def test_adaptive_chunk_follows_the_resident_size(monkeypatch):
     assert small == 64 and big == 4 and 4 <= mid <= 64 and small >= mid >= big
     fixed = serving.Server(1 << 40, max_slots=16, precision="fp64", chunk=7)
     assert fixed.chunk_steps(1000) == 7 and fixed.chunk_steps(64 << 20) == 7
+
+
+def test_guard_puts_requests_past_the_guard_first_oldest_first(monkeypatch):
+    """The "guard" policy orders as "hrrn" until a request has waited longer than the
+    guard; then the requests past it go first in arrival order."""
+    monkeypatch.setattr(serving, "CavityPool", FakePool)
+    big1, big2, small, mid = requests([(6, 4, 400), (6, 4, 300), (4, 2, 10), (6, 4, 20)])
+    big1.arrival, big2.arrival, small.arrival, mid.arrival = 0.0, 1.0, 9.0, 9.5
+    reqs = [big1, big2, small, mid]
+    srv = serving.Server(1 << 40, max_slots=16, precision="fp64", policy="guard", guard_s=8.5)
+    hr = serving.Server(1 << 40, max_slots=16, precision="fp64", policy="hrrn")
+    pend = [2, 3, 1, 0]
+    # at t = 9.6 both large requests have waited past 8.5 s: oldest first, then hrrn
+    assert srv.order_pending(pend, reqs, 9.6) == [0, 1, 2, 3]
+    # at t = 9.2 only the first has
+    assert srv.order_pending(pend, reqs, 9.2)[0] == 0
+    assert srv.order_pending(pend, reqs, 9.2)[1:] == [i for i in hr.order_pending(pend, reqs, 9.2) if i != 0]
+    # no request past the guard: the hrrn order itself
+    early = serving.Server(1 << 40, max_slots=16, precision="fp64", policy="guard", guard_s=100.0)
+    assert early.order_pending(pend, reqs, 9.6) == hr.order_pending(pend, reqs, 9.6)
+    # default guard: guard_services x the mean estimated service time given
+    auto = serving.Server(1 << 40, max_slots=16, precision="fp64", policy="guard", guard_services=2.0)
+    assert auto.order_pending(pend, reqs, 9.6, mean_service_s=4.0)[:2] == [0, 1]   # guard 8 s
+    assert auto.order_pending(pend, reqs, 9.6, mean_service_s=4.5)[0] == 0        # guard 9 s
+    assert auto.order_pending(pend, reqs, 9.6, mean_service_s=5.0) == hr.order_pending(pend, reqs, 9.6)
+
+
+def test_guard_completes_every_request_under_the_node_limit(fake):
+    reqs = requests(SIZES)
+    sat = 300_000
+    srv = serving.Server(1 << 40, max_slots=16, precision="fp64", chunk=4, policy="guard",
+                         saturation_nodes=sat, guard_s=0.0)
+    results, _ = srv.run(reqs, time_scale=0.0)
+    srv.close()
+    assert all(r is not None for r in results)
+    for npts, _, resident, running_before in fake[0].log:
+        assert resident <= sat or running_before == 0
+    # a zero guard admits in arrival order: first come, first served
+    assert [x[0] for x in fake[0].log] == [r.npts for r in reqs]
