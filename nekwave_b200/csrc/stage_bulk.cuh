@@ -170,7 +170,7 @@ __device__ __forceinline__ bool bulk_wait_tile(const StageParams& P, unsigned ch
 // flight.  VROW: the r-derivative's node rows read with 16-byte loads.  Dc: D where
 // the t contraction of CONSTD reads it (a parameter copy).
 template <int N, int GEO, int KS, int EPB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool VROW = false>
+          bool VROW = false, bool ILP2 = false>
 __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, unsigned char* smem,
                                           const int tid, const double* Dc) {
     static_assert(GEO != GEO_NODAL, "per-element geometry and connections");
@@ -195,7 +195,8 @@ __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, un
     const ElemGeo* sg = reinterpret_cast<const ElemGeo*>(smem + L::geo0);
     const int* sc = reinterpret_cast<const int*>(smem + L::conn0) + ((e0 * 6) & 3);
     double* sflux = reinterpret_cast<double*>(smem + L::flux0);
-    compute2<N, GEO, false, KS, EPB, true, false, CONSTD, EARLY, false, DSMEM, CtaBar, L::CSR, KSM, VROW>(
+    compute2<N, GEO, false, KS, EPB, true, false, CONSTD, EARLY, false, DSMEM, CtaBar, L::CSR, KSM, VROW,
+             ILP2>(
         P, e0, su, sg, sc, sD, sflux, nullptr, tid, G, Dc, CtaBar(), sk);
 }
 
@@ -219,20 +220,20 @@ __device__ __forceinline__ int bulk_tile_index(const StageParams& P, int b) {
 }
 
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL, bool VROW>
+          bool ZCOL, bool VROW, bool ILP2>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage_bulk_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int t = bulk_tile_index<EPB, ZCOL>(P, blockIdx.x);
-    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW>(P, t * EPB, smem, threadIdx.x, P.Dc);
+    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW, ILP2>(P, t * EPB, smem, threadIdx.x, P.Dc);
 }
 
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL, bool VROW>
+          bool ZCOL, bool VROW, bool ILP2>
 cudaError_t launch_bulk(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int threads = EPB * KS * N * N;
-    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL, VROW>;
+    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL, VROW, ILP2>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, L::total, KSM ? 1 : 0, MINB};
     static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
     if (cudaError_t e = set_smem_once(kern, L::total, attr_set); e != cudaSuccess) return e;

@@ -84,13 +84,14 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
             } else if constexpr (v.alg >= 1000) {
                 // the bulk-copy one-tile form (stage_bulk.cuh), second-family flags
                 // ALG - 1000: 2 SPLIT (required), 8 CONSTD, 16 EARLY, 32 KSM, 64 DSMEM,
-                // 1 ZCOL (z-column tile order on structured boxes), 4 VROW (16-byte row loads)
+                // 1 ZCOL (z-column tile order on structured boxes), 4 VROW (16-byte row
+                // loads), 128 ILP2 (two partial sums per derivative)
                 constexpr int fl = v.alg - 1000;
-                static_assert((fl & 2) != 0 && v.ks == 2 && fl < 128, "the field split");
+                static_assert((fl & 2) != 0 && v.ks == 2 && fl < 256, "the field split");
                 if constexpr (GEO == GEO_BOX && !F32)
                     return launch_bulk<NWB_N, GEO, v.ks, v.epb, v.minb, (fl & 8) != 0, (fl & 64) != 0,
-                                       (fl & 32) != 0, (fl & 16) != 0, (fl & 1) != 0, (fl & 4) != 0>(
-                        p, st, cfg);
+                                       (fl & 32) != 0, (fl & 16) != 0, (fl & 1) != 0, (fl & 4) != 0,
+                                       (fl & 128) != 0>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == kFirstGeneral) {

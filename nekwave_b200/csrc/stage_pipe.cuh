@@ -498,10 +498,12 @@ __device__ __forceinline__ void row_pairs(const double* p, double (&r)[N]) {
 // VROW (FP64 field split on unpadded tiles whose components and elements start on
 // 16-byte boundaries for even N: the bulk-copy tile): the r-derivative's node rows
 // are read with 16-byte loads (row_pairs), half the shared loads of that sum.  The
-// arithmetic and its order are unchanged.
+// arithmetic and its order are unchanged.  ILP2 (axis-aligned field split): each
+// derivative sum is formed as two partial sums (even and odd l) added at the end,
+// two independent FMA chains per sum instead of one (a different rounding order).
 template <int N, int GEO, bool F32, int KS, int EPB, bool SPLIT, bool PAD, bool CONSTD = false,
           bool EARLY = false, bool FACEDONE = false, bool DSMEM = false, class Bar = CtaBar,
-          int CSX = 0, bool KSM = false, bool VROW = false>
+          int CSX = 0, bool KSM = false, bool VROW = false, bool ILP2 = false>
 __device__ __forceinline__ void compute2(const StageParams& P, const int e0, const double* su,
                                          const ElemGeo* sg, const int* sc, const double* sD,
                                          double* sflux, unsigned char* smem_uc, const int tid,
@@ -742,20 +744,29 @@ __device__ __forceinline__ void compute2(const StageParams& P, const int e0, con
                     row_pairs<N>(V + 2 * CS + PP * k + RP * j, rowz);
                     row_pairs<N>(V + 1 * CS + PP * k + RP * j, rowy);
                 }
+                // ILP2: odd l into a second set of partial sums, added at the end
+                TX Wz_r = 0, Wy_r = 0, Wz_s = 0, Wx_s = 0, Wy_t = 0, Wx_t = 0;
 #pragma unroll
                 for (int l = 0; l < N; ++l) {
                     const TX dr = (DSMEM || !SAME) ? static_cast<TX>(sD[i + l * N]) : static_cast<TX>(Dr[l]);
                     const TX ds = (DSMEM || !SAME) ? static_cast<TX>(sD[j + l * N]) : static_cast<TX>(Ds[l]);
                     const TX dt = CONSTD ? static_cast<TX>(Dc[k + l * N]) : static_cast<TX>(sD[k + l * N]);
                     const int is = PP * k + RP * l + i;
+                    const bool odd = ILP2 && (l & 1);
+                    TX& az_r = odd ? Wz_r : Vz_r; TX& ay_r = odd ? Wy_r : Vy_r;
+                    TX& az_s = odd ? Wz_s : Vz_s; TX& ax_s = odd ? Wx_s : Vx_s;
+                    TX& ay_t = odd ? Wy_t : Vy_t; TX& ax_t = odd ? Wx_t : Vx_t;
                     if constexpr (VROW) {
-                        Vz_r += dr * rowz[l]; Vy_r += dr * rowy[l];
+                        az_r += dr * rowz[l]; ay_r += dr * rowy[l];
                     } else {
                         const int ir = PP * k + RP * j + l;
-                        Vz_r += dr * V[2 * CS + ir]; Vy_r += dr * V[1 * CS + ir];
+                        az_r += dr * V[2 * CS + ir]; ay_r += dr * V[1 * CS + ir];
                     }
-                    Vz_s += ds * V[2 * CS + is]; Vx_s += ds * V[0 * CS + is];
-                    Vy_t += dt * col[1][l]; Vx_t += dt * col[0][l];
+                    az_s += ds * V[2 * CS + is]; ax_s += ds * V[0 * CS + is];
+                    ay_t += dt * col[1][l]; ax_t += dt * col[0][l];
+                }
+                if constexpr (ILP2) {
+                    Vz_r += Wz_r; Vy_r += Wy_r; Vz_s += Wz_s; Vx_s += Wx_s; Vy_t += Wy_t; Vx_t += Wx_t;
                 }
                 const TX rx = met(0), sy = met(4), tz = met(8);
                 rhs[0] = sgn * static_cast<double>(sy * Vz_s - tz * Vy_t);
