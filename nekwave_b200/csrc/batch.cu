@@ -258,7 +258,7 @@ template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, M
 // EARLY = neighbour traces requested while the tile's copies fly.  VROW = the
 // r-derivative's node rows read with 16-byte loads.
 template <int N> struct NBulk { static constexpr bool on = false, VROW = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1; };
-template <> struct NBulk<5> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 4; };
+template <> struct NBulk<5> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 8; };
 template <> struct NBulk<6> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3; };
 template <> struct NBulk<7> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4; };
 template <> struct NBulk<9> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2; };
@@ -311,9 +311,8 @@ template <int N, bool F32>
 cudaError_t launch_n(int stage, const SlotDev* slots, const WorkItem* work, int ntiles, int dry,
                      const double* Dh, cudaStream_t st, int* epb_out) {
     using Sh = NShape<N>;
-    if (epb_out) *epb_out = Sh::EPB;
+    if (epb_out) *epb_out = (NBulk<N>::on && !F32) ? NBulk<N>::EPB : Sh::EPB;
     if constexpr (NBulk<N>::on && !F32) {
-        static_assert(NBulk<N>::EPB == Sh::EPB, "the per-N work list is cut with NShape's EPB");
         DParam dp{};
         if constexpr (NBulk<N>::CD) {
             if (Dh) {
@@ -507,11 +506,18 @@ cudaError_t launch_batch_stage_n(int N, int f32, int stage, const SlotDev* slots
     }
 }
 
-int batch_epb_n(int N) {
+namespace {
+template <int N>
+int epb_n(int f32) {
+    return (NBulk<N>::on && !f32) ? NBulk<N>::EPB : NShape<N>::EPB;
+}
+}  // namespace
+
+int batch_epb_n(int N, int f32) {
     switch (N) {
-        case 2: return NShape<2>::EPB; case 3: return NShape<3>::EPB; case 4: return NShape<4>::EPB;
-        case 5: return NShape<5>::EPB; case 6: return NShape<6>::EPB; case 7: return NShape<7>::EPB;
-        case 8: return NShape<8>::EPB; case 9: return NShape<9>::EPB; case 10: return NShape<10>::EPB;
+        case 2: return epb_n<2>(f32); case 3: return epb_n<3>(f32); case 4: return epb_n<4>(f32);
+        case 5: return epb_n<5>(f32); case 6: return epb_n<6>(f32); case 7: return epb_n<7>(f32);
+        case 8: return epb_n<8>(f32); case 9: return epb_n<9>(f32); case 10: return epb_n<10>(f32);
         default: return 1;
     }
 }

@@ -54,13 +54,13 @@ cudaError_t launch_batch_stage(int f32, int stage, const SlotDev* slots, const W
                                const int* ntiles, int* counters, int grid, int smem, int dry,
                                cudaStream_t st);
 // Per-N mode: one block per tile of the given N (work points at that N's tiles,
-// which must have been cut with batch_epb_n(N) elements each).  Dh: that N's D on
+// which must have been cut with batch_epb_n(N, f32) elements each).  Dh: that N's D on
 // the host when every resident cavity of that N shares it (lets the kernel take D
 // from its parameters), else null.
 cudaError_t launch_batch_stage_n(int N, int f32, int stage, const SlotDev* slots,
                                  const WorkItem* work, int ntiles, int dry, const double* Dh,
                                  cudaStream_t st);
-int batch_epb_n(int N);
+int batch_epb_n(int N, int f32);
 // Diagnostics after a step (post = 1) or of the initial state (post = 0):
 // energy partials per tile and probe values into the slots' history buffers.
 // only_slot >= 0 restricts the work to one slot (initial-state diagnostics).

@@ -259,7 +259,7 @@ struct nwb_pool {
         std::vector<nwb::WorkItem> wn;
         for (int N = 2; N <= 10; ++N) {
             n_off[N] = static_cast<int>(wn.size());
-            const int epb = nwb::batch_epb_n(N);
+            const int epb = nwb::batch_epb_n(N, f32);
             for (int s = 0; s < max_slots; ++s) {
                 const SlotHost& h = slots[s];
                 if (!h.used || h.N != N) continue;
@@ -408,7 +408,7 @@ nwb_status nwb_pool_create(size_t hbm_budget_bytes, int max_slots, nwb_precision
     if (e == cudaSuccess) {
         double min_tile = 1e300;
         for (int N = 2; N <= 10; ++N) {
-            const int epb = std::min(nwb::batch_shape(N, p->f32).epb, nwb::batch_epb_n(N));
+            const int epb = std::min(nwb::batch_shape(N, p->f32).epb, nwb::batch_epb_n(N, p->f32));
             min_tile = std::min(min_tile, 144.0 * N * N * N * epb);
         }
         const double cap = static_cast<double>(max_slots) + static_cast<double>(hbm_budget_bytes) / min_tile + 1;
