@@ -256,12 +256,33 @@ template <> struct NShape<10> { static constexpr int KS = 2, EPB = 1, KSM = 0, M
 // FP64 per-N shapes that run the bulk-copy one-tile form (the single-mesh default
 // at these N): k staged in shared memory, CD = t-derivative D from the parameters.
 // EARLY = neighbour traces requested while the tile's copies fly.  VROW = the
-// r-derivative's node rows read with 16-byte loads.
-template <int N> struct NBulk { static constexpr bool on = false, VROW = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1; };
-template <> struct NBulk<5> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 8; };
-template <> struct NBulk<6> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3; };
-template <> struct NBulk<7> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4; };
-template <> struct NBulk<9> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2; };
+// r-derivative's node rows read with 16-byte loads.  AHEAD = 1: each block pulls
+// into L2 the tile of the block half a wave of resident blocks after it (PoolPull).
+template <int N> struct NBulk { static constexpr bool on = false, VROW = false, CD = false, EARLY = false; static constexpr int EPB = 1, MINB = 1, AHEAD = 0; };
+template <> struct NBulk<5> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 8, AHEAD = 0; };
+template <> struct NBulk<6> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 2, MINB = 3, AHEAD = 1; };
+template <> struct NBulk<7> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 4, AHEAD = 0; };
+template <> struct NBulk<9> { static constexpr bool on = true, VROW = false, CD = true, EARLY = true; static constexpr int EPB = 1, MINB = 2, AHEAD = 1; };
+
+// Thread 0's L2 pull in a per-N bulk kernel: the tile of the work item about AHEAD/2
+// waves of resident blocks after this block's (that N's tiles are the grid, one per
+// block, in work-list order), in whichever cavity it lies.
+template <int N>
+struct PoolPull {
+    const SlotDev* slots;
+    const WorkItem* work;
+    int stage;
+    __device__ __forceinline__ void operator()() const {
+        const int b = stage::tile_ahead<NBulk<N>::AHEAD, NBulk<N>::MINB>(blockIdx.x);
+        if (b < 0) return;
+        const WorkItem w = work[b];
+        const SlotDev& S = slots[w.slot];
+        if (!S.active) return;
+        constexpr long long N3 = N * N * N;
+        stage::prefetch_nodes_l2(S.u[S.par ^ (stage & 1)], S.k, S.stride, w.e0 * N3,
+                                 min(NBulk<N>::EPB, S.nelt - w.e0) * N3);
+    }
+};
 
 template <int N, bool CD>
 __global__ void __launch_bounds__(NBulk<N>::EPB * 2 * N * N, NBulk<N>::MINB)
@@ -272,8 +293,12 @@ batch_bulk_n_kernel(const SlotDev* __restrict__ slots, const WorkItem* __restric
     const SlotDev& S = slots[w.slot];
     if (!S.active) return;
     const StageParams P = slot_params(S, stage, dry);
-    stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY, NBulk<N>::VROW>(P, w.e0, smem,
-                                                                                      threadIdx.x, dp.d);
+    if constexpr (NBulk<N>::AHEAD > 0)
+        stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY, NBulk<N>::VROW>(
+            P, w.e0, smem, threadIdx.x, dp.d, PoolPull<N>{slots, work, stage});
+    else
+        stage::bulk_tile<N, GEO_BOX, 2, NBulk<N>::EPB, CD, false, true, NBulk<N>::EARLY, NBulk<N>::VROW>(
+            P, w.e0, smem, threadIdx.x, dp.d);
 }
 
 template <int N, bool CD>

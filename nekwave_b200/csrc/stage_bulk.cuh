@@ -168,11 +168,13 @@ __device__ __forceinline__ bool bulk_wait_tile(const StageParams& P, unsigned ch
 // EARLY: the neighbour traces of the face phase are requested from global memory
 // (through the box structure when there is one) while the tile's copies are in
 // flight.  VROW: the r-derivative's node rows read with 16-byte loads.  Dc: D where
-// the t contraction of CONSTD reads it (a parameter copy).
+// the t contraction of CONSTD reads it (a parameter copy).  pull: called by thread 0
+// right after it has issued the tile's copies (NoPull, or a functor that pulls a
+// later block's tile into L2).
 template <int N, int GEO, int KS, int EPB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool VROW = false, bool ILP2 = false>
+          bool VROW = false, bool ILP2 = false, class Pull = NoPull>
 __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, unsigned char* smem,
-                                          const int tid, const double* Dc) {
+                                          const int tid, const double* Dc, const Pull& pull = Pull()) {
     static_assert(GEO != GEO_NODAL, "per-element geometry and connections");
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int NT = EPB * KS * N * N;
@@ -186,7 +188,10 @@ __device__ __forceinline__ void bulk_tile(const StageParams& P, const int e0, un
     __syncthreads();
     const long long g0 = static_cast<long long>(e0) * L::N3;
     FaceGather<face_points_per_thread<N, KS>()> G;
-    if (tid == 0) bulk_issue<N, EPB, KSM>(P, e0, smem);
+    if (tid == 0) {
+        bulk_issue<N, EPB, KSM>(P, e0, smem);
+        pull();
+    }
     if constexpr (EARLY) gather2<N, GEO, KS, EPB, false, false>(P, e0, nullptr, nullptr, tid, G);
     if (!bulk_wait_tile<N, EPB, KSM>(P, smem, tid)) return;
     const int off = static_cast<int>(g0 & 1);
@@ -219,21 +224,43 @@ __device__ __forceinline__ int bulk_tile_index(const StageParams& P, int b) {
     return b;
 }
 
+// Thread 0's L2 pull of the single-mesh kernel: the tile of the block that starts
+// about AHEAD/2 waves of resident blocks after this one (tile_ahead), in the same
+// tile order.
+template <int N3, int EPB, int MINB, int AHEAD, bool ZCOL>
+struct MeshPull {
+    const StageParams& P;
+    __device__ __forceinline__ void operator()() const {
+        const int b = tile_ahead<AHEAD, MINB>(blockIdx.x);
+        if (b < 0) return;
+        const int e = bulk_tile_index<EPB, ZCOL>(P, b) * EPB;
+        prefetch_tile_l2<N3>(P, e, min(EPB, P.nelt - e));
+    }
+};
+
+// AHEAD (0, 1, 2): block b also pulls into L2 the tile of the block that starts
+// about AHEAD/2 waves of resident blocks later, so that block's bulk copies read L2
+// instead of DRAM; 0: no pull.  On B200 this pays where few blocks are resident
+// (6 and 9 points: 3 and 2 per SM), whose tile waits the other blocks hide least.
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL, bool VROW, bool ILP2>
+          bool ZCOL, bool VROW, bool ILP2, int AHEAD>
 __global__ void __launch_bounds__(EPB * KS * N * N, MINB)
     stage_bulk_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int t = bulk_tile_index<EPB, ZCOL>(P, blockIdx.x);
-    bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW, ILP2>(P, t * EPB, smem, threadIdx.x, P.Dc);
+    if constexpr (AHEAD > 0)
+        bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW, ILP2>(
+            P, t * EPB, smem, threadIdx.x, P.Dc, MeshPull<N * N * N, EPB, MINB, AHEAD, ZCOL>{P});
+    else
+        bulk_tile<N, GEO, KS, EPB, CONSTD, DSMEM, KSM, EARLY, VROW, ILP2>(P, t * EPB, smem, threadIdx.x, P.Dc);
 }
 
 template <int N, int GEO, int KS, int EPB, int MINB, bool CONSTD, bool DSMEM, bool KSM, bool EARLY,
-          bool ZCOL, bool VROW, bool ILP2>
+          bool ZCOL, bool VROW, bool ILP2, int AHEAD = 0>
 cudaError_t launch_bulk(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     using L = BulkLayout<N, EPB, KSM>;
     constexpr int threads = EPB * KS * N * N;
-    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL, VROW, ILP2>;
+    auto kern = stage_bulk_kernel<N, GEO, KS, EPB, MINB, CONSTD, DSMEM, KSM, EARLY, ZCOL, VROW, ILP2, AHEAD>;
     if (cfg) *cfg = StageConfig{KS, EPB, threads, L::total, KSM ? 1 : 0, MINB};
     static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
     if (cudaError_t e = set_smem_once(kern, L::total, attr_set); e != cudaSuccess) return e;

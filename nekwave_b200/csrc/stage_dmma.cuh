@@ -109,10 +109,11 @@ __device__ __forceinline__ void dmma8_planes(const StageParams& P, const double*
 // kernel's parameter copy when the caller has one (constant-bank operands), else
 // the tile's shared copy at smem + DmmaLayout8::D (the same values either way).
 // All threads of the block call it; threads beyond 64*WPF take part in the
-// barriers only.
+// barriers only.  e_ahead >= 0: thread 0 also pulls the u_in and k of that element
+// into L2, for the block that loads it later.
 template <int WPF>
 __device__ __forceinline__ void dmma8_tile(const StageParams& P, const int e, unsigned char* smem,
-                                           const int tid, const double* Dc) {
+                                           const int tid, const double* Dc, const int e_ahead = -1) {
     constexpr int N = 8, N3 = 512, NT = 64 * WPF;
     static_assert(WPF == 1 || WPF == 2, "one or two warps per field");
     using L = DmmaLayout8;
@@ -125,6 +126,7 @@ __device__ __forceinline__ void dmma8_tile(const StageParams& P, const int e, un
     if (tid < NT) {
         issue2<N, GEO_BOX, 1, NT, false>(P, e, su, sg, sc, tid);
         if (tid < 64) cp_async8(sD + tid, P.D + tid);
+        if (tid == 0 && e_ahead >= 0) prefetch_tile_l2<N3>(P, e_ahead, 1);
     }
     cp_async_commit();
     cp_async_wait<0>();
@@ -163,16 +165,19 @@ __device__ __forceinline__ void dmma8_tile(const StageParams& P, const int e, un
     }
 }
 
-template <int MINB, int WPF>
+// AHEAD (0, 1, 2): block e also pulls into L2 the element of the block that starts
+// about AHEAD/2 waves of resident blocks later (tile_ahead); 0: no prefetch.
+template <int MINB, int WPF, int AHEAD>
 __global__ void __launch_bounds__(64 * WPF, MINB) stage_dmma8_kernel(const __grid_constant__ StageParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    dmma8_tile<WPF>(P, blockIdx.x, smem, threadIdx.x, P.Dc);
+    const int e_ahead = AHEAD > 0 ? tile_ahead<(AHEAD > 0 ? AHEAD : 1), MINB>(blockIdx.x) : -1;
+    dmma8_tile<WPF>(P, blockIdx.x, smem, threadIdx.x, P.Dc, e_ahead);
 }
 
-template <int MINB, int WPF = 1>
+template <int MINB, int WPF = 1, int AHEAD = 0>
 cudaError_t launch_dmma8(const StageParams* p, cudaStream_t st, StageConfig* cfg) {
     constexpr int smem = DmmaLayout8::total;
-    auto kern = stage_dmma8_kernel<MINB, WPF>;
+    auto kern = stage_dmma8_kernel<MINB, WPF, AHEAD>;
     if (cfg) *cfg = StageConfig{WPF, 1, 64 * WPF, smem, 0, MINB};
     static std::atomic<int> attr_set[kMaxDeviceSlots];  // per kernel and device
     if (cudaError_t e = set_smem_once(kern, smem, attr_set); e != cudaSuccess) return e;

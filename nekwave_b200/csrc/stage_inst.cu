@@ -29,7 +29,9 @@ constexpr Shape kShapes[] = {NWB_VLIST(NWB_X)};
 #undef NWB_X
 constexpr int kNumShapes = static_cast<int>(sizeof(kShapes) / sizeof(Shape));
 // FP64 tensor-core shapes and the bulk-copy form: axis-aligned class, FP64 only
-constexpr bool fp64_only(int alg) { return alg == 1 || alg == 200 || alg == 201 || alg >= 1000; }
+constexpr bool fp64_only(int alg) {
+    return alg == 1 || alg == 200 || alg == 201 || alg == 211 || alg == 212 || alg >= 1000;
+}
 constexpr int count_simt() {
     int n = 0;
     for (int i = 0; i < kNumShapes; ++i) n += !fp64_only(kShapes[i].alg);
@@ -70,6 +72,13 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                     return launch_dmma8<v.minb, v.alg - 199>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
+            } else if constexpr (v.alg == 211 || v.alg == 212) {
+                // two warps per field, each block pulling a later block's element into
+                // L2 half (211) or one (212) wave of resident blocks ahead
+                if constexpr (GEO == GEO_BOX && !F32 && NWB_N == 8)
+                    return launch_dmma8<v.minb, 2, v.alg - 210>(p, st, cfg);
+                else
+                    return cudaErrorInvalidValue;
             } else if constexpr (v.alg >= 2 && v.alg <= 129) {
                 static_assert(v.ksm == 0, "second family: k from L2");
                 constexpr int fl = v.alg - 2;
@@ -85,13 +94,15 @@ cudaError_t launch_variant(int vid, const StageParams* p, cudaStream_t st, Stage
                 // the bulk-copy one-tile form (stage_bulk.cuh), second-family flags
                 // ALG - 1000: 2 SPLIT (required), 8 CONSTD, 16 EARLY, 32 KSM, 64 DSMEM,
                 // 1 ZCOL (z-column tile order on structured boxes), 4 VROW (16-byte row
-                // loads), 128 ILP2 (two partial sums per derivative)
+                // loads), 128 ILP2 (two partial sums per derivative), 256 / 512 AHEAD
+                // (the tile of a block half / one wave of resident blocks later pulled
+                // into L2)
                 constexpr int fl = v.alg - 1000;
-                static_assert((fl & 2) != 0 && v.ks == 2 && fl < 256, "the field split");
+                static_assert((fl & 2) != 0 && v.ks == 2 && fl < 1024 && (fl & 768) != 768, "the field split");
                 if constexpr (GEO == GEO_BOX && !F32)
                     return launch_bulk<NWB_N, GEO, v.ks, v.epb, v.minb, (fl & 8) != 0, (fl & 64) != 0,
                                        (fl & 32) != 0, (fl & 16) != 0, (fl & 1) != 0, (fl & 4) != 0,
-                                       (fl & 128) != 0>(p, st, cfg);
+                                       (fl & 128) != 0, (fl & 512) ? 2 : ((fl & 256) ? 1 : 0)>(p, st, cfg);
                 else
                     return cudaErrorInvalidValue;
             } else if constexpr (GEO == GEO_BOX || I == kFirstGeneral) {

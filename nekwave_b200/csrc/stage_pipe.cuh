@@ -58,6 +58,53 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 
+// Number of SM identifiers of the GPU (%nsmid: at least the number of SMs).
+__device__ __forceinline__ int sm_ids() {
+    unsigned n;
+    asm("mov.u32 %0, %%nsmid;\n" : "=r"(n));
+    return static_cast<int>(n);
+}
+
+// Tile of the block that starts about AHEAD/2 waves of resident blocks after block
+// b (a wave = the SMs times the MINB resident blocks per SM), or -1 past the grid.
+// The hardware hands out blocks in index order, so that block runs about half a
+// (AHEAD = 1) or one (AHEAD = 2) block lifetime later.
+template <int AHEAD, int MINB>
+__device__ __forceinline__ int tile_ahead(int b) {
+    const long long a = static_cast<long long>(b) + static_cast<long long>(sm_ids()) * MINB * AHEAD / 2;
+    return a < static_cast<long long>(gridDim.x) ? static_cast<int>(a) : -1;
+}
+
+// Nodes [g0, g0 + cnt) of the six components of u and of k (component stride S)
+// pulled into L2 by twelve bulk prefetches (one thread; nothing waits on them), for
+// the block that will load them later: its own copies then read L2 instead of DRAM.
+// The ranges are rounded out to 16-byte boundaries, which stay inside the state
+// arrays (components are 512-byte aligned and padded to 64 doubles).
+__device__ __forceinline__ void prefetch_nodes_l2(const double* u, const double* k, long long S,
+                                                  long long g0, long long cnt) {
+    const long long a0 = g0 & ~1ll, a1 = (g0 + cnt + 1) & ~1ll;
+    const unsigned bytes = static_cast<unsigned>((a1 - a0) * 8);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(u + c * S + a0), "r"(bytes)
+                     : "memory");
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(k + c * S + a0), "r"(bytes)
+                     : "memory");
+}
+
+// The u_in and k of the tile of elements [e0, e0 + n) pulled into L2.
+template <int N3>
+__device__ __forceinline__ void prefetch_tile_l2(const StageParams& P, int e0, int n) {
+    prefetch_nodes_l2(P.u_in, P.k, P.stride, static_cast<long long>(e0) * N3, static_cast<long long>(n) * N3);
+}
+
+// The no-op L2 pull of a tile function (see bulk_tile).
+struct NoPull {
+    __device__ __forceinline__ void operator()() const {}
+};
+
 // FP32-bulk, affine classes: an element runs the FP64 column arithmetic when the
 // largest deviation of its tile from the per-element linear fit exceeds this
 // fraction of the largest deviation from its centre value (in any component).
