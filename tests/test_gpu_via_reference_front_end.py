@@ -130,7 +130,7 @@ def test_device_diagnostics_front_end_on_a_nonzero_wave(gpu, tmp_path):
         p = d / "case.json"
         p.write_text(json.dumps(c))
         r = subprocess.run([exe, str(p), str(comp), repr(x0), repr(y0), repr(z0), repr(sig)],
-                           capture_output=True, text=True, timeout=420, cwd=d)
+                           capture_output=True, text=True, timeout=240, cwd=d)
         assert r.returncode == 0, name + ": " + r.stdout[-2000:] + r.stderr[-2000:]
         sim = [ln for ln in r.stdout.splitlines() if ln.startswith("[pulse-case] simulate_s")]
         hist = [[float(v) for v in row] for row in list(csv.reader(open(d / "out" / "energy_history.csv")))[1:]]
