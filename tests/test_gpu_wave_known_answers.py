@@ -1,13 +1,18 @@
-"""The plane-wave known answer of the reference's convergence study on libnwb
+"""Known answers of the reference on libnwb (tests/known_answers.py).
+
+The plane wave of the reference's convergence study
 (examples/numerical_analysis/convergence_test/convergence_test.cpp: a TEM wave in a
 periodic box, h-refinement at degree 4 and p-refinement at 3..8 points, central and
-upwind flux; one period here): each run equals the oracle's (pinned to the
-reference's own build) to the step-parity tolerance, and the errors against the
-analytic wave converge as the study expects (tests/plane_wave.py)."""
+upwind flux; one period here) and the cavity modes of its regression cases
+tests/3dboxpec_test and tests/3dboxper_test (box meshes in place of their missing
+NekCEM meshes): each run equals the oracle's (pinned to the reference's own build) to
+the step-parity tolerance, and its error against the analytic fields is what the
+study and the cases expect.
+"""
 import pytest
 
 from oracle import oracle as O
-from tests import plane_wave as W
+from tests import known_answers as W
 from tests.gpu_helpers import record, rel_l2, solver_for
 
 pytestmark = pytest.mark.gpu
@@ -46,3 +51,21 @@ def test_plane_wave_convergence_matches_the_oracle_and_the_analytic_wave(gpu, c0
             assert all(a > b for a, b in zip(errs, errs[1:])), errs
             assert errs[-1] < 1e-6, errs
     record(f"plane_wave_c0_{c0:g}.json", rows)
+
+
+@pytest.mark.parametrize("name", ["3dboxpec", "3dboxper"])
+def test_regression_cavity_modes_under_the_reference_threshold(gpu, name):
+    m = W.mode_mesh(name, 4)
+    dt = W.mode_dt(m)
+    u0 = W.mode_exact(name, m, 0.0)
+    s = solver_for(m, 0.0)
+    s.uploadState(u0)
+    s.steps(dt, W.MODE_STEPS)
+    got = s.downloadState()
+    s.finalize()
+    want, _ = O.step(m, 0.0, dt, W.MODE_STEPS, u0)
+    d = rel_l2(got, want)
+    err = W.mode_rel_l2(m, got, W.MODE_STEPS * dt, name)
+    record(f"mode_{name}.json", dict(rel_l2_vs_oracle=d, rel_l2_vs_exact=err, steps=W.MODE_STEPS))
+    assert d < STEPS_TOL, d
+    assert err <= W.MODE_THRESHOLD, err
