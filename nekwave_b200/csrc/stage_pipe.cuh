@@ -67,8 +67,9 @@ __device__ __forceinline__ int sm_ids() {
 
 // Tile of the block that starts about AHEAD/2 waves of resident blocks after block
 // b (a wave = the SMs times the MINB resident blocks per SM), or -1 past the grid.
-// The hardware hands out blocks in index order, so that block runs about half a
-// (AHEAD = 1) or one (AHEAD = 2) block lifetime later.
+// Blocks are handed out in about index order, so that block starts about half a
+// (AHEAD = 1) or one (AHEAD = 2) block lifetime later; the order is not guaranteed,
+// and a pull that misses only costs L2 traffic.
 template <int AHEAD, int MINB>
 __device__ __forceinline__ int tile_ahead(int b) {
     const long long a = static_cast<long long>(b) + static_cast<long long>(sm_ids()) * MINB * AHEAD / 2;
