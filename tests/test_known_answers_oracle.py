@@ -1,7 +1,7 @@
 """CPU: the oracle on the known answers of the reference (tests/known_answers.py): the
 plane wave of its convergence study (one period, h- and p-refinement, central and
 upwind flux) and the cavity modes of its two regression cases.  The GPU path is held
-to the same answers in test_gpu_known_answers.py."""
+to the same answers in test_gpu_validation_against_known_answers.py."""
 import pytest
 
 from oracle import oracle as O
